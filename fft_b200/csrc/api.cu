@@ -1,0 +1,715 @@
+// api.cu -- the C-ABI (include/gofft.h): device-resident plans and the
+// reference-facing entry points that mirror go-fft/fft's Go API.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <sstream>
+
+#include "../../include/gofft.h"
+#include "plan.cuh"
+
+using namespace gf;
+
+#define GF_CK(x)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess)                                                              \
+      return set_err(GOFFT_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+struct gofft_plan {
+  int kind = GOFFT_C2C, prec = F64, rank = 1;
+  std::vector<long long> shape;
+  long long batch = 1, istride = 1, idist = 0, ostride = 1, odist = 0, total = 1;
+  std::vector<std::shared_ptr<const Exec1D>> ax;  // complex exec per axis
+  std::shared_ptr<const ExecReal> rx;             // real exec of the last axis (R2C)
+  long long chunk = 1;                            // images per L2 block (rank-2 R2C)
+  size_t ws_bytes = 0;
+  void *ws = nullptr;
+  void *d_in = nullptr, *d_out = nullptr;
+  size_t d_in_bytes = 0, d_out_bytes = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  int device = 0;
+  bool cached = false;
+  ~gofft_plan() {
+    if (ws) cudaFree(ws);
+    if (d_in) cudaFree(d_in);
+    if (d_out) cudaFree(d_out);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+static const char *kVersion = "gofft-b200 0.1 (sm_100a)";
+
+extern "C" const char *gofft_last_error(void) { return last_err(); }
+extern "C" const char *gofft_version(void) { return kVersion; }
+
+// ---------------------------------------------------------------------------
+// Plan construction
+// ---------------------------------------------------------------------------
+static long long env_ll(const char *name, long long dflt) {
+  const char *v = getenv(name);
+  if (!v || !*v) return dflt;
+  return atoll(v);
+}
+
+// Extent (elements) of `batch` lines of `len` elements at (dist, stride).
+static long long extent(long long batch, long long dist, long long len, long long stride) {
+  if (batch <= 0 || len <= 0) return 0;
+  return (batch - 1) * dist + (len - 1) * stride + 1;
+}
+
+static int plan_ws(gofft_plan *p) {
+  size_t need = 0;
+  if (p->kind == GOFFT_C2C) {
+    for (int a = 0; a < p->rank; a++) {
+      const long long lines = (p->rank == 1 ? p->batch : p->batch * (p->total / p->shape[a]));
+      need = std::max(need, p->ax[a]->ws_bytes(lines));
+    }
+  } else if (p->rank == 1) {
+    need = p->rx->ws_bytes(p->batch);
+  } else {
+    const long long rows = p->shape[0], rc = p->shape[1] / 2 + 1;
+    const size_t cols_buf = (size_t)rows * rc * p->chunk * csize(p->prec) + 256;
+    need = cols_buf + std::max(p->rx->ws_bytes(rows * p->chunk), p->ax[0]->ws_bytes(rc * p->chunk));
+  }
+  p->ws_bytes = need;
+  if (need) {
+    cudaError_t e = cudaMalloc(&p->ws, need);
+    if (e != cudaSuccess) return set_err(GOFFT_ENOMEM, std::string("workspace: ") + cudaGetErrorString(e));
+  }
+  return 0;
+}
+
+extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, int rank,
+                                 int64_t batch, int64_t istride, int64_t idist, int64_t ostride,
+                                 int64_t odist, gofft_plan **out) {
+  if (!out) return set_err(GOFFT_EINVAL, "null output handle");
+  *out = nullptr;
+  if (kind != GOFFT_C2C && kind != GOFFT_R2C) return set_err(GOFFT_EINVAL, "bad kind");
+  if (precision < 0 || precision > 2) return set_err(GOFFT_EINVAL, "bad precision");
+  if (rank < 1 || rank > 16 || !shape) return set_err(GOFFT_EINVAL, "rank must be in [1,16]");
+  if (batch < 1) return set_err(GOFFT_EINVAL, "batch must be >= 1");
+  for (int a = 0; a < rank; a++)
+    if (shape[a] <= 0) return set_err(GOFFT_EINVAL, "fft: shape lengths must be positive");
+  if (kind == GOFFT_R2C && rank > 2) return set_err(GOFFT_EUNSUPPORTED, "real transforms support rank 1 and 2");
+  std::unique_ptr<gofft_plan> p(new gofft_plan());
+  p->kind = kind;
+  p->prec = precision;
+  p->rank = rank;
+  p->batch = batch;
+  cudaGetDevice(&p->device);
+  p->shape.assign(shape, shape + rank);
+  p->total = 1;
+  for (long long s : p->shape) p->total *= s;
+  const long long last = p->shape[rank - 1];
+  const long long rc = last / 2 + 1;
+  const long long in_line = kind == GOFFT_C2C ? p->total : p->total;            // reals or complex
+  const long long out_line = kind == GOFFT_C2C ? p->total : p->total / last * rc;  // bins
+  p->istride = istride > 0 ? istride : 1;
+  p->ostride = ostride > 0 ? ostride : 1;
+  p->idist = idist > 0 ? idist : in_line * p->istride;
+  p->odist = odist > 0 ? odist : out_line * p->ostride;
+  if (rank > 1 && (p->istride != 1 || p->ostride != 1))
+    return set_err(GOFFT_EUNSUPPORTED, "rank > 1 needs unit element strides");
+  if (kind == GOFFT_C2C) {
+    for (int a = 0; a < rank; a++) {
+      auto ex = get_exec(p->shape[a], precision);
+      if (!ex) return GOFFT_ECUDA;
+      p->ax.push_back(ex);
+    }
+  } else {
+    p->rx = get_real(last, precision);
+    if (!p->rx) return GOFFT_ECUDA;
+    if (rank == 2) {
+      auto ex = get_exec(p->shape[0], precision);
+      if (!ex) return GOFFT_ECUDA;
+      p->ax.push_back(ex);
+      if (p->istride != 1 || p->idist != p->total || p->ostride != 1 || p->odist != p->shape[0] * rc)
+        return set_err(GOFFT_EUNSUPPORTED, "2-D real transforms need contiguous images");
+      // images per block: keep a block's complex intermediate L2-resident
+      const long long budget = env_ll("GOFFT_L2_BLOCK_BYTES", 48ll << 20);
+      const long long per = p->shape[0] * rc * (long long)csize(precision);
+      p->chunk = std::max<long long>(1, std::min<long long>(batch, budget / std::max<long long>(1, per)));
+    }
+  }
+  if (int rc2 = plan_ws(p.get())) return rc2;
+  GF_CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  *out = p.release();
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_plan_destroy(gofft_plan *p) {
+  if (!p) return GOFFT_OK;
+  if (p->cached) return GOFFT_OK;  // memoised plans live for the process
+  delete p;
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_plan_workspace_size(const gofft_plan *p, size_t *bytes) {
+  if (!p || !bytes) return set_err(GOFFT_EINVAL, "null argument");
+  *bytes = p->ws_bytes;
+  return GOFFT_OK;
+}
+
+extern "C" int64_t gofft_plan_describe(const gofft_plan *p, char *buf, int64_t cap) {
+  if (!p) return -1;
+  std::ostringstream o;
+  o << "{\"kind\":\"" << (p->kind == GOFFT_C2C ? "c2c" : "r2c") << "\",\"precision\":" << p->prec
+    << ",\"batch\":" << p->batch << ",\"shape\":[";
+  for (int a = 0; a < p->rank; a++) o << (a ? "," : "") << p->shape[a];
+  o << "],\"workspace\":" << p->ws_bytes << ",\"chunk\":" << p->chunk << ",\"axes\":[";
+  for (size_t a = 0; a < p->ax.size(); a++) o << (a ? "," : "") << p->ax[a]->describe();
+  o << "]";
+  if (p->rx) o << ",\"real\":" << p->rx->describe();
+  o << "}";
+  const std::string s = o.str();
+  if (buf && cap > 0) {
+    const size_t k = std::min<size_t>(s.size(), (size_t)cap - 1);
+    memcpy(buf, s.data(), k);
+    buf[k] = 0;
+  }
+  return (int64_t)s.size();
+}
+
+extern "C" int64_t gofft_plan_table(const gofft_plan *p, int which, int64_t *out, int64_t cap) {
+  if (!p || p->kind != GOFFT_C2C || p->rank != 1) return -1;
+  const Exec1D &e = *p->ax[0];
+  std::vector<int64_t> v;
+  if ((which == 0 || which == 1) && e.kind == K_RADER) {
+    std::vector<int> t(e.n - 1);
+    if (cudaMemcpy(t.data(), which == 0 ? e.perm : e.iperm, t.size() * sizeof(int),
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+      return -1;
+    v.assign(t.begin(), t.end());
+  } else if (which == 2 && e.kind == K_BLUE) {
+    v.resize(e.n);
+    if (cudaMemcpy(v.data(), e.jj, v.size() * sizeof(long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return -1;
+  } else if (which == 3 && e.kind == K_RADER) {
+    v = {e.g, e.cl};
+  } else if (which == 4 && e.kind == K_BLUE) {
+    v = {e.m};
+  } else {
+    return -1;
+  }
+  if (out)
+    for (int64_t i = 0; i < (int64_t)v.size() && i < cap; i++) out[i] = v[i];
+  return (int64_t)v.size();
+}
+
+// ---------------------------------------------------------------------------
+// Execution on device pointers
+// ---------------------------------------------------------------------------
+static int exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, cudaStream_t st) {
+  const int cj = inverse ? 1 : 0;
+  if (p->rank == 1) {
+    const double sc = inverse ? 1.0 / (double)p->shape[0] : 1.0;
+    return p->ax[0]->exec(mk_side((void *)in, p->idist, 0, p->istride, 1),
+                          mk_side(out, p->odist, 0, p->ostride, 1), p->batch, cj, cj, sc, p->ws, st);
+  }
+  const size_t c = csize(p->prec);
+  const bool merged = p->idist == p->total && p->odist == p->total;
+  const long long nb = merged ? 1 : p->batch;
+  const long long per = merged ? p->batch : 1;
+  for (long long b = 0; b < nb; b++) {
+    const char *src = (const char *)in + (size_t)b * p->idist * c;
+    char *dst = (char *)out + (size_t)b * p->odist * c;
+    bool first = true;
+    long long inner = p->total;
+    for (int a = 0; a < p->rank; a++) {
+      const long long L = p->shape[a];
+      inner /= L;
+      if (L == 1) continue;
+      const Side sd_in = mk_side(first ? (void *)src : (void *)dst, L * inner, 1, inner, inner);
+      const Side sd_out = mk_side(dst, L * inner, 1, inner, inner);
+      const long long lines = per * (p->total / L);
+      const double sc = inverse ? 1.0 / (double)L : 1.0;
+      if (int rc = p->ax[a]->exec(sd_in, sd_out, lines, cj, cj, sc, p->ws, st)) return rc;
+      first = false;
+    }
+    if (first && src != dst) GF_CK(cudaMemcpyAsync(dst, src, (size_t)per * p->total * c, cudaMemcpyDeviceToDevice, st));
+  }
+  return GOFFT_OK;
+}
+
+static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st) {
+  if (p->rank == 1) {
+    return p->rx->r2c(mk_side((void *)in, p->idist, 0, p->istride, 1), mk_side(out, p->odist, 0, p->ostride, 1),
+                      p->batch, p->ws, st);
+  }
+  const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
+  const size_t r = rsize(p->prec), c = csize(p->prec);
+  char *wsx = (char *)p->ws + (((size_t)rows * rc * p->chunk * c + 255) & ~(size_t)255);
+  for (long long b0 = 0; b0 < p->batch; b0 += p->chunk) {
+    const long long nb = std::min(p->chunk, p->batch - b0);
+    const char *src = (const char *)in + (size_t)b0 * rows * cols * r;
+    char *dst = (char *)out + (size_t)b0 * rows * rc * c;
+    // rows: real transform along the last axis (rfft2.go:41-51)
+    if (int e = p->rx->r2c(contig((void *)src, cols), contig(dst, rc), nb * rows, wsx, st)) return e;
+    // columns: complex transform down each of the rc columns (rfft2.go:53-72)
+    if (rows > 1) {
+      const Side cs = mk_side(dst, rows * rc, 1, rc, rc);
+      if (int e = p->ax[0]->exec(cs, cs, nb * rc, 0, 0, 1.0, wsx, st)) return e;
+    }
+  }
+  return GOFFT_OK;
+}
+
+static int exec_c2r(gofft_plan *p, const void *in, long long nbins, void *out, cudaStream_t st) {
+  const long long last = p->shape[p->rank - 1], rc = last / 2 + 1;
+  if (nbins <= 0 || nbins > rc) nbins = rc;
+  if (p->rank == 1) {
+    return p->rx->c2r(mk_side((void *)in, p->idist, 0, p->istride, 1), (int)nbins,
+                      mk_side(out, p->odist, 0, p->ostride, 1), p->batch, 1.0, p->ws, st);
+  }
+  // 2-D: in (complex) is the plan's output side; out (real) its input side
+  const long long rows = p->shape[0], cols = last;
+  const size_t r = rsize(p->prec), c = csize(p->prec);
+  char *colbuf = (char *)p->ws;
+  char *wsx = colbuf + (((size_t)rows * rc * p->chunk * c + 255) & ~(size_t)255);
+  for (long long b0 = 0; b0 < p->batch; b0 += p->chunk) {
+    const long long nb = std::min(p->chunk, p->batch - b0);
+    const char *src = (const char *)in + (size_t)b0 * rows * rc * c;
+    char *dst = (char *)out + (size_t)b0 * rows * cols * r;
+    // columns: complex inverse, normalised by 1/rows (rfft2.go:100-120)
+    const Side cin = mk_side((void *)src, rows * rc, 1, rc, rc);
+    const Side cout = mk_side(colbuf, rows * rc, 1, rc, rc);
+    if (int e = p->ax[0]->exec(cin, cout, nb * rc, 1, 1, 1.0 / (double)rows, wsx, st)) return e;
+    // rows: real inverse of length cols (rfft2.go:122-136)
+    if (int e = p->rx->c2r(contig(colbuf, rc), (int)rc, contig(dst, cols), nb * rows, 1.0, wsx, st)) return e;
+  }
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, gofft_stream stream) {
+  if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_C2C) return set_err(GOFFT_EINVAL, "plan is not complex-to-complex");
+  return exec_c2c(p, in, out, inverse, (cudaStream_t)stream);
+}
+extern "C" int gofft_exec_r2c(gofft_plan *p, const void *in, void *out, gofft_stream stream) {
+  if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_R2C) return set_err(GOFFT_EINVAL, "plan is not real");
+  return exec_r2c(p, in, out, (cudaStream_t)stream);
+}
+extern "C" int gofft_exec_c2r(gofft_plan *p, const void *in, int64_t nbins, void *out, gofft_stream stream) {
+  if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_R2C) return set_err(GOFFT_EINVAL, "plan is not real");
+  return exec_c2r(p, in, nbins, out, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Host-pointer execution
+// ---------------------------------------------------------------------------
+static int ensure_staging(gofft_plan *p, size_t in_b, size_t out_b) {
+  if (p->d_in_bytes < in_b) {
+    if (p->d_in) cudaFree(p->d_in);
+    p->d_in = nullptr;
+    p->d_in_bytes = 0;
+    cudaError_t e = cudaMalloc(&p->d_in, in_b);
+    if (e != cudaSuccess) return set_err(GOFFT_ENOMEM, "staging buffer");
+    p->d_in_bytes = in_b;
+  }
+  if (p->d_out_bytes < out_b) {
+    if (p->d_out) cudaFree(p->d_out);
+    p->d_out = nullptr;
+    p->d_out_bytes = 0;
+    cudaError_t e = cudaMalloc(&p->d_out, out_b);
+    if (e != cudaSuccess) return set_err(GOFFT_ENOMEM, "staging buffer");
+    p->d_out_bytes = out_b;
+  }
+  return 0;
+}
+
+static size_t c2c_bytes(const gofft_plan *p, bool in) {
+  const long long d = in ? p->idist : p->odist, s = in ? p->istride : p->ostride;
+  const long long el = p->rank == 1 ? extent(p->batch, d, p->total, s) : (p->batch - 1) * d + p->total;
+  return (size_t)el * csize(p->prec);
+}
+static size_t real_bytes(const gofft_plan *p) {
+  const long long el = p->rank == 1 ? extent(p->batch, p->idist, p->total, p->istride) : p->batch * p->total;
+  return (size_t)el * rsize(p->prec);
+}
+static size_t bins_bytes(const gofft_plan *p) {
+  const long long rc = p->shape[p->rank - 1] / 2 + 1;
+  const long long el = p->rank == 1 ? extent(p->batch, p->odist, rc, p->ostride)
+                                    : p->batch * (p->total / p->shape[p->rank - 1]) * rc;
+  return (size_t)el * csize(p->prec);
+}
+
+static int host_run(gofft_plan *p, const void *in, size_t in_b, void *out, size_t out_b, int which,
+                    int inverse, long long nbins) {
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (int rc = ensure_staging(p, in_b, out_b)) return rc;
+  GF_CK(cudaMemcpyAsync(p->d_in, in, in_b, cudaMemcpyHostToDevice, p->stream));
+  int rc = 0;
+  if (which == 0) rc = exec_c2c(p, p->d_in, p->d_out, inverse, p->stream);
+  else if (which == 1) rc = exec_r2c(p, p->d_in, p->d_out, p->stream);
+  else rc = exec_c2r(p, p->d_in, nbins, p->d_out, p->stream);
+  if (rc) return rc;
+  GF_CK(cudaMemcpyAsync(out, p->d_out, out_b, cudaMemcpyDeviceToHost, p->stream));
+  GF_CK(cudaStreamSynchronize(p->stream));
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_exec_c2c_host(gofft_plan *p, const void *in, void *out, int inverse) {
+  if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_C2C) return set_err(GOFFT_EINVAL, "plan is not complex-to-complex");
+  return host_run(p, in, c2c_bytes(p, true), out, c2c_bytes(p, false), 0, inverse, 0);
+}
+extern "C" int gofft_exec_r2c_host(gofft_plan *p, const void *in, void *out) {
+  if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_R2C) return set_err(GOFFT_EINVAL, "plan is not real");
+  return host_run(p, in, real_bytes(p), out, bins_bytes(p), 1, 0, 0);
+}
+extern "C" int gofft_exec_c2r_host(gofft_plan *p, const void *in, int64_t nbins, void *out) {
+  if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_R2C) return set_err(GOFFT_EINVAL, "plan is not real");
+  return host_run(p, in, bins_bytes(p), out, real_bytes(p), 2, 0, nbins);
+}
+
+// ---------------------------------------------------------------------------
+// Reference-facing entry points (FP64, host buffers)
+// ---------------------------------------------------------------------------
+static gofft_plan *make_1d(int kind, long long n) {
+  gofft_plan *p = nullptr;
+  const int64_t sh[1] = {n};
+  if (gofft_plan_create(kind, GOFFT_F64, sh, 1, 1, 1, 0, 1, 0, &p) != GOFFT_OK) return nullptr;
+  return p;
+}
+
+extern "C" int gofft_new_plan(int64_t n, gofft_plan **out) {
+  if (!out) return set_err(GOFFT_EINVAL, "null output handle");
+  if (n < 0) return set_err(GOFFT_EINVAL, "fft: negative length");
+  gofft_plan *p = nullptr;
+  if (n == 0) {
+    p = new gofft_plan();
+    p->shape = {0};
+    p->total = 0;
+  } else {
+    p = make_1d(GOFFT_C2C, n);
+    if (!p) return GOFFT_ECUDA;
+  }
+  *out = p;
+  return GOFFT_OK;
+}
+
+// Memoised plans keyed by length (plan.go:283-317 / rfft.go:48-64): built
+// outside the lock, first store wins.
+static gofft_plan *memo(std::map<long long, gofft_plan *> &m, std::mutex &mu, long long n, bool real) {
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = m.find(n);
+    if (it != m.end()) return it->second;
+  }
+  gofft_plan *p = nullptr;
+  if (real) {
+    p = make_1d(GOFFT_R2C, n);
+  } else if (gofft_new_plan(n, &p) != GOFFT_OK) {
+    p = nullptr;
+  }
+  if (!p) return nullptr;
+  p->cached = true;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = m.find(n);
+  if (it != m.end()) {
+    p->cached = false;
+    delete p;
+    return it->second;
+  }
+  m[n] = p;
+  return p;
+}
+static std::mutex g_cmu, g_rmu;
+static std::map<long long, gofft_plan *> g_cplans, g_rplans;
+
+extern "C" int gofft_cached_plan(int64_t n, gofft_plan **out) {
+  if (!out) return set_err(GOFFT_EINVAL, "null output handle");
+  if (n < 0) return set_err(GOFFT_EINVAL, "fft: negative length");
+  *out = memo(g_cplans, g_cmu, n, false);
+  return *out ? GOFFT_OK : GOFFT_ECUDA;
+}
+
+extern "C" int64_t gofft_plan_len(const gofft_plan *p) { return p ? (p->shape.empty() ? 0 : p->shape.back()) : 0; }
+
+static int plan_c2c_host(gofft_plan *p, double *dst, const double *src, int inverse) {
+  if (!p || (!dst && p->total) || (!src && p->total)) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->total == 0) return GOFFT_OK;
+  if (p->kind != GOFFT_C2C || p->rank != 1 || p->batch != 1) return set_err(GOFFT_EINVAL, "not a 1-D complex plan");
+  return gofft_exec_c2c_host(p, src, dst, inverse);
+}
+extern "C" int gofft_plan_fft(gofft_plan *p, double *dst, const double *src) { return plan_c2c_host(p, dst, src, 0); }
+extern "C" int gofft_plan_ifft(gofft_plan *p, double *dst, const double *src) { return plan_c2c_host(p, dst, src, 1); }
+
+extern "C" int gofft_new_real_plan(int64_t n, gofft_plan **out) {
+  if (!out) return set_err(GOFFT_EINVAL, "null output handle");
+  if (n < 0) return set_err(GOFFT_EINVAL, "fft: negative length");
+  gofft_plan *p = nullptr;
+  if (n == 0) {
+    p = new gofft_plan();
+    p->kind = GOFFT_R2C;
+    p->shape = {0};
+    p->total = 0;
+  } else {
+    p = make_1d(GOFFT_R2C, n);
+    if (!p) return GOFFT_ECUDA;
+  }
+  *out = p;
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_real_plan_rfft(gofft_plan *p, double *dst, const double *src) {
+  if (!p) return set_err(GOFFT_EINVAL, "null plan");
+  if (p->total == 0) return GOFFT_OK;
+  if (p->kind != GOFFT_R2C || p->rank != 1 || p->batch != 1) return set_err(GOFFT_EINVAL, "not a 1-D real plan");
+  if (!dst || !src) return set_err(GOFFT_EINVAL, "null argument");
+  return gofft_exec_r2c_host(p, src, dst);
+}
+
+extern "C" int gofft_real_plan_irfft(gofft_plan *p, double *dst, const double *src, int64_t nsrc) {
+  if (!p) return set_err(GOFFT_EINVAL, "null plan");
+  if (p->total == 0) return GOFFT_OK;
+  if (p->kind != GOFFT_R2C || p->rank != 1 || p->batch != 1) return set_err(GOFFT_EINVAL, "not a 1-D real plan");
+  if (!dst) return set_err(GOFFT_EINVAL, "null argument");
+  const long long rc = p->total / 2 + 1;
+  long long nb = std::min<long long>(std::max<long long>(nsrc, 0), rc);
+  if (nb > 0 && !src) return set_err(GOFFT_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (int e = ensure_staging(p, (size_t)rc * 16, (size_t)p->total * 8)) return e;
+  if (nb > 0) GF_CK(cudaMemcpyAsync(p->d_in, src, (size_t)nb * 16, cudaMemcpyHostToDevice, p->stream));
+  if (int e = p->rx->c2r(contig(p->d_in, rc), (int)nb, contig(p->d_out, p->total), 1, 1.0, p->ws, p->stream)) return e;
+  GF_CK(cudaMemcpyAsync(dst, p->d_out, (size_t)p->total * 8, cudaMemcpyDeviceToHost, p->stream));
+  GF_CK(cudaStreamSynchronize(p->stream));
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_fft(const double *x, int64_t n, double *out) {
+  if (n < 0) return set_err(GOFFT_EINVAL, "fft: negative length");
+  if (n <= 1) {
+    if (n == 1) memmove(out, x, 16);
+    return GOFFT_OK;
+  }
+  gofft_plan *p = nullptr;
+  if (int e = gofft_cached_plan(n, &p)) return e;
+  return gofft_plan_fft(p, out, x);
+}
+extern "C" int gofft_ifft(const double *x, int64_t n, double *out) {
+  if (n < 0) return set_err(GOFFT_EINVAL, "fft: negative length");
+  if (n <= 1) {
+    if (n == 1) memmove(out, x, 16);
+    return GOFFT_OK;
+  }
+  gofft_plan *p = nullptr;
+  if (int e = gofft_cached_plan(n, &p)) return e;
+  return gofft_plan_ifft(p, out, x);
+}
+extern "C" int gofft_fft_real(const double *x, int64_t n, double *out) {
+  if (n < 0) return set_err(GOFFT_EINVAL, "fft: negative length");
+  std::vector<double> c((size_t)2 * n, 0.0);
+  for (int64_t i = 0; i < n; i++) c[2 * i] = x[i];
+  return gofft_fft(c.data(), n, out);
+}
+
+extern "C" int gofft_rfft(const double *x, int64_t n, double *out) {
+  if (n < 0) return set_err(GOFFT_EINVAL, "fft: negative length");
+  if (n == 0) return GOFFT_OK;
+  gofft_plan *p = memo(g_rplans, g_rmu, n, true);
+  if (!p) return GOFFT_ECUDA;
+  return gofft_real_plan_rfft(p, out, x);
+}
+extern "C" int gofft_irfft(const double *spectrum, int64_t nspec, int64_t n, double *out) {
+  if (n <= 0) return GOFFT_OK;
+  gofft_plan *p = memo(g_rplans, g_rmu, n, true);
+  if (!p) return GOFFT_ECUDA;
+  return gofft_real_plan_irfft(p, out, spectrum, nspec);
+}
+
+// N-D plans memoised by (kind, shape).
+static std::mutex g_nmu;
+static std::map<std::pair<int, std::vector<long long>>, gofft_plan *> g_nplans;
+static gofft_plan *nd_plan(int kind, const std::vector<long long> &shape) {
+  auto key = std::make_pair(kind, shape);
+  {
+    std::lock_guard<std::mutex> lk(g_nmu);
+    auto it = g_nplans.find(key);
+    if (it != g_nplans.end()) return it->second;
+  }
+  gofft_plan *p = nullptr;
+  std::vector<int64_t> sh(shape.begin(), shape.end());
+  if (gofft_plan_create(kind, GOFFT_F64, sh.data(), (int)sh.size(), 1, 1, 0, 1, 0, &p) != GOFFT_OK) return nullptr;
+  p->cached = true;
+  std::lock_guard<std::mutex> lk(g_nmu);
+  auto it = g_nplans.find(key);
+  if (it != g_nplans.end()) {
+    p->cached = false;
+    delete p;
+    return it->second;
+  }
+  g_nplans[key] = p;
+  return p;
+}
+
+// ndfft.go:50-62
+static int validate_shape(const int64_t *shape, int rank, int64_t len) {
+  long long prod = 1;
+  for (int a = 0; a < rank; a++) {
+    if (shape[a] <= 0) return set_err(GOFFT_EINVAL, "fft: shape lengths must be positive");
+    prod *= shape[a];
+  }
+  if (prod != len) return set_err(GOFFT_EINVAL, "fft: shape product does not match len(data)");
+  return GOFFT_OK;
+}
+
+static int fftn_impl(const double *data, int64_t len, const int64_t *shape, int rank, double *out, int inverse) {
+  if (rank < 0 || (rank > 0 && !shape)) return set_err(GOFFT_EINVAL, "bad rank");
+  if (int e = validate_shape(shape, rank, len)) return e;
+  if (len <= 1) {
+    if (len == 1) memmove(out, data, 16);
+    return GOFFT_OK;
+  }
+  gofft_plan *p = nd_plan(GOFFT_C2C, std::vector<long long>(shape, shape + rank));
+  if (!p) return GOFFT_ECUDA;
+  return gofft_exec_c2c_host(p, data, out, inverse);
+}
+extern "C" int gofft_fftn(const double *data, int64_t len, const int64_t *shape, int rank, double *out) {
+  return fftn_impl(data, len, shape, rank, out, 0);
+}
+extern "C" int gofft_ifftn(const double *data, int64_t len, const int64_t *shape, int rank, double *out) {
+  return fftn_impl(data, len, shape, rank, out, 1);
+}
+extern "C" int gofft_fft2(const double *data, int64_t len, int64_t rows, int64_t cols, double *out) {
+  const int64_t sh[2] = {rows, cols};
+  return fftn_impl(data, len, sh, 2, out, 0);
+}
+extern "C" int gofft_ifft2(const double *data, int64_t len, int64_t rows, int64_t cols, double *out) {
+  const int64_t sh[2] = {rows, cols};
+  return fftn_impl(data, len, sh, 2, out, 1);
+}
+
+extern "C" int gofft_rfft2(const double *data, int64_t len, int64_t rows, int64_t cols, double *out) {
+  if (rows <= 0 || cols <= 0) return set_err(GOFFT_EINVAL, "fft: shape lengths must be positive");
+  if (rows * cols != len) return set_err(GOFFT_EINVAL, "fft: shape product does not match len(data)");
+  gofft_plan *p = nd_plan(GOFFT_R2C, {rows, cols});
+  if (!p) return GOFFT_ECUDA;
+  return gofft_exec_r2c_host(p, data, out);
+}
+
+extern "C" int gofft_irfft2(const double *data, int64_t len, int64_t rows, int64_t cols, double *out) {
+  if (rows <= 0 || cols <= 0) return set_err(GOFFT_EINVAL, "fft: shape lengths must be positive");
+  const long long need = rows * (cols / 2 + 1);
+  gofft_plan *p = nd_plan(GOFFT_R2C, {rows, cols});
+  if (!p) return GOFFT_ECUDA;
+  if (len >= need) return gofft_exec_c2r_host(p, data, 0, out);
+  // short spectrum: missing bins are zero (rfft2.go:94-99)
+  std::vector<double> pad((size_t)need * 2, 0.0);
+  if (len > 0) memcpy(pad.data(), data, (size_t)len * 16);
+  return gofft_exec_c2r_host(p, pad.data(), 0, out);
+}
+
+// window.go:20-22, 59-78
+extern "C" int gofft_hann(int64_t n, double *out) {
+  if (n <= 0) return GOFFT_OK;
+  if (n == 1) {
+    out[0] = 1;
+    return GOFFT_OK;
+  }
+  const double denom = (double)(n - 1);
+  for (int64_t k = 0; k < n; k++) out[k] = 0.5 + (-1.0) * 0.5 * cos(2 * M_PI * 1.0 * (double)k / denom);
+  return GOFFT_OK;
+}
+
+// Spectrogram frames on device buffers (freq.go:107-127 for even segments).
+static int spectro_dev(int prec, const void *x, int64_t nx, int64_t seg, int64_t overlap, const void *win,
+                       double d, void *out, int64_t frames, cudaStream_t st) {
+  if (frames <= 0) return GOFFT_OK;
+  const long long m = seg / 2;
+  auto rx = get_real(seg, prec);
+  if (!rx) return GOFFT_ECUDA;
+  if (rx->mode != R_PACKED_FUSED) return set_err(GOFFT_EUNSUPPORTED, "segment too long for the fused spectrogram");
+  KArgs a{};
+  a.in = mk_side((void *)x, seg - overlap, 0, 1, 1);
+  a.out = mk_side(out, m + 1, 0, 1, 1);
+  a.aux0 = rx->tw2;
+  a.aux1 = win;
+  a.scale = d / (double)seg;
+  (void)nx;
+  return launch_line(OP_SPECTRO, *rx->cx->prog, a, frames, st);
+}
+
+static int64_t frame_count(int64_t nx, int64_t seg, int64_t overlap) {
+  const int64_t step = seg - overlap;
+  if (nx < seg) return 0;
+  return (nx - seg) / step + 1;
+}
+
+extern "C" int gofft_spectrogram_device(int precision, const void *x, int64_t nx, int64_t segment,
+                                        int64_t overlap, const void *window, double d, void *out,
+                                        int64_t *nframes, gofft_stream stream) {
+  if (segment <= 0) return set_err(GOFFT_EINVAL, "fft: segment length must be positive");
+  if (overlap < 0 || overlap >= segment) return set_err(GOFFT_EINVAL, "fft: overlap must satisfy 0 <= overlap < segment");
+  if (segment % 2) return set_err(GOFFT_EUNSUPPORTED, "device spectrogram needs an even segment");
+  if (precision < 0 || precision > 2) return set_err(GOFFT_EINVAL, "bad precision");
+  const int64_t frames = frame_count(nx, segment, overlap);
+  if (nframes) *nframes = frames;
+  if (!out) return GOFFT_OK;
+  return spectro_dev(precision, x, nx, segment, overlap, window, d, out, frames, (cudaStream_t)stream);
+}
+
+// PSD (freq.go:69-90) of one host signal.
+extern "C" int gofft_psd(const double *x, int64_t n, double d, double *out) {
+  if (n <= 0) return GOFFT_OK;
+  const int64_t m = n / 2 + 1;
+  std::vector<double> spec((size_t)2 * m);
+  if (int e = gofft_rfft(x, n, spec.data())) return e;
+  const double scale = d / (double)n;
+  for (int64_t k = 0; k < m; k++) {
+    const double re = spec[2 * k], im = spec[2 * k + 1];
+    double pw = (re * re + im * im) * scale;
+    if (k != 0 && !(n % 2 == 0 && k == m - 1)) pw *= 2;
+    out[k] = pw;
+  }
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_spectrogram(const double *x, int64_t nx, int64_t segment, int64_t overlap,
+                                 const double *window, int64_t nwindow, double d, double *out,
+                                 int64_t *nframes) {
+  if (segment <= 0) return set_err(GOFFT_EINVAL, "fft: segment length must be positive");
+  if (nwindow != segment) return set_err(GOFFT_EINVAL, "fft: window length must equal segment length");
+  if (overlap < 0 || overlap >= segment) return set_err(GOFFT_EINVAL, "fft: overlap must satisfy 0 <= overlap < segment");
+  const int64_t frames = frame_count(nx, segment, overlap);
+  if (nframes) *nframes = frames;
+  if (!out || frames == 0) return GOFFT_OK;
+  const int64_t bins = segment / 2 + 1;
+  if (segment % 2 == 0 && get_real(segment, F64) && get_real(segment, F64)->mode == R_PACKED_FUSED) {
+    void *dx = nullptr, *dw = nullptr, *dout = nullptr;
+    const size_t used = (size_t)((frames - 1) * (segment - overlap) + segment);
+    int rc = GOFFT_OK;
+    if (cudaMalloc(&dx, used * 8) != cudaSuccess || cudaMalloc(&dw, segment * 8) != cudaSuccess ||
+        cudaMalloc(&dout, (size_t)frames * bins * 8) != cudaSuccess) {
+      rc = set_err(GOFFT_ENOMEM, "spectrogram buffers");
+    } else {
+      cudaMemcpy(dx, x, used * 8, cudaMemcpyHostToDevice);
+      cudaMemcpy(dw, window, segment * 8, cudaMemcpyHostToDevice);
+      rc = spectro_dev(F64, dx, nx, segment, overlap, dw, d, dout, frames, 0);
+      if (rc == GOFFT_OK) {
+        cudaError_t e = cudaMemcpy(out, dout, (size_t)frames * bins * 8, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = set_err(GOFFT_ECUDA, cudaGetErrorString(e));
+      }
+    }
+    cudaFree(dx);
+    cudaFree(dw);
+    cudaFree(dout);
+    return rc;
+  }
+  // odd (or over-long) segments: one PSD per windowed frame
+  std::vector<double> seg((size_t)segment);
+  for (int64_t t = 0; t < frames; t++) {
+    const int64_t start = t * (segment - overlap);
+    for (int64_t i = 0; i < segment; i++) seg[i] = x[start + i] * window[i];
+    if (int e = gofft_psd(seg.data(), segment, d, out + t * bins)) return e;
+  }
+  return GOFFT_OK;
+}

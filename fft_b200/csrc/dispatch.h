@@ -1,0 +1,72 @@
+// dispatch.h -- host-visible handles to the per-precision kernel instances.
+#pragma once
+#include <cuda_runtime.h>
+#include "engine.cuh"
+
+namespace gf {
+
+enum Prec { F64 = 0, F32 = 1, F32C = 2 };
+enum Op {
+  OP_C2C = 0,      // plain complex line
+  OP_C2C_TW = 1,   // four-step pass 1 (twiddled epilogue)
+  OP_R2C = 2,      // even real forward (packed)
+  OP_C2R = 3,      // even real inverse (packed)
+  OP_R2C_FULL = 4, // real forward through a full complex line
+  OP_C2R_FULL = 5, // real inverse through the Hermitian mirror
+  OP_RADER = 6,    // fused Rader convolution
+  OP_BLUE = 7,     // fused Bluestein convolution
+  OP_SPECTRO = 8,  // fused spectrogram frame
+  OP_COUNT = 9
+};
+
+typedef void (*KFn)(KArgs);
+
+// Line kernel for (maxe, op) in each precision; nullptr if not instantiated.
+KFn line_kernel_f64(int maxe, int op);
+KFn line_kernel_f32(int maxe, int op);
+KFn line_kernel_f32c(int maxe, int op);
+
+// Elementwise / table kernels of one precision, launched on `st`.
+struct EwArgs {
+  long long nlines;
+  int len, ldst, off, p;
+  const int *perm;
+  const void *chirp;  // sp_t table
+  int cj;
+  double scale;
+  void *x0s, *dc;
+};
+
+#define GF_DECLARE_PREC(SUFFIX)                                                               \
+  namespace prec_##SUFFIX {                                                                   \
+  cudaError_t gather(void *dst, const Side &src, const EwArgs &e, cudaStream_t st);           \
+  cudaError_t spec_mul(void *y, const void *B, const EwArgs &e, cudaStream_t st);             \
+  cudaError_t rader_scatter(const Side &dst, const void *y, const int *iperm, const EwArgs &e, \
+                            cudaStream_t st);                                                 \
+  cudaError_t blue_unchirp(const Side &dst, const void *y, const EwArgs &e, cudaStream_t st); \
+  cudaError_t scatter(const Side &dst, const void *src, const EwArgs &e, cudaStream_t st);    \
+  cudaError_t stage_tw(void *tw, const StageTab &t, long long total, cudaStream_t st);        \
+  cudaError_t roots(void *tw, long long L, long long count, cudaStream_t st);                 \
+  cudaError_t spectrum(void *dst, const double2 *src, double s, long long n, cudaStream_t st); \
+  cudaError_t untangle(const Side &dst, const void *Z, long long nl, int m, const void *tw,   \
+                       cudaStream_t st);                                                      \
+  cudaError_t reverse_untangle(void *Z, const Side &src, long long nl, int m, int nb,         \
+                               const void *tw, cudaStream_t st);                              \
+  cudaError_t promote(void *dst, const Side &src, long long nl, int n, cudaStream_t st);      \
+  cudaError_t copy_bins(const Side &dst, const void *src, long long nl, int n, cudaStream_t st); \
+  cudaError_t mirror(void *dst, const Side &src, long long nl, int n, int nb, cudaStream_t st); \
+  cudaError_t take_real(const Side &dst, const void *src, long long nl, int n, double scale,  \
+                        cudaStream_t st);                                                     \
+  }
+// Plan-time integer and chirp tables (FP64 / exact integer work).
+cudaError_t gen_rader_perm(int *perm, int *iperm, long long p, long long g, cudaStream_t st);
+cudaError_t gen_rader_kernel(double2 *b, const int *perm, long long p, long long cl, int cyclic,
+                             cudaStream_t st);
+cudaError_t gen_chirp(long long *jj, double2 *w, long long n, cudaStream_t st);
+cudaError_t gen_blue_kernel(double2 *b, const double2 *w, long long n, long long m, cudaStream_t st);
+
+GF_DECLARE_PREC(f64)
+GF_DECLARE_PREC(f32)
+GF_DECLARE_PREC(f32c)
+
+}  // namespace gf

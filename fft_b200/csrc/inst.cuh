@@ -1,0 +1,123 @@
+// inst.cuh -- instantiates every kernel of one precision (included by the
+// per-precision translation units so the three compile in parallel).
+#pragma once
+#include "dispatch.h"
+#include "kernels.cuh"
+
+namespace gf {
+
+template <class P, int M> KFn pick_line(int op) {
+  switch (op) {
+    case OP_C2C: return k_line<P, M, OpC2C>;
+    case OP_C2C_TW: return k_line<P, M, OpC2CTwiddle>;
+    case OP_R2C: return k_line<P, M, OpR2CPacked>;
+    case OP_C2R: return k_line<P, M, OpC2RPacked>;
+    case OP_R2C_FULL: return k_line<P, M, OpR2CFull>;
+    case OP_C2R_FULL: return k_line<P, M, OpC2RFull>;
+    case OP_RADER: return k_line<P, M, OpRader>;
+    case OP_BLUE: return k_line<P, M, OpBluestein>;
+    case OP_SPECTRO: return k_line<P, M, OpSpectro>;
+    default: return nullptr;
+  }
+}
+
+// FP64 lines use 16 register elements per thread (32 would spill); the FP32
+// forms also get a 32-element variant for lines longer than 16 x 512.
+template <class P> KFn pick_maxe(int maxe, int op) {
+  if (maxe == 16) return pick_line<P, 16>(op);
+  if constexpr (sizeof(typename P::cpx) == 8) {
+    if (maxe == 32) return pick_line<P, 32>(op);
+  }
+  return nullptr;
+}
+
+static inline int ew_blocks(long long total) {
+  long long b = (total + 255) / 256;
+  if (b > 148 * 32) b = 148 * 32;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace gf
+
+#define GF_DEFINE_PREC(P, SUFFIX)                                                              \
+  namespace gf {                                                                               \
+  KFn line_kernel_##SUFFIX(int maxe, int op) {                                                 \
+    return pick_maxe<P>(maxe, op);                                                             \
+  }                                                                                            \
+  namespace prec_##SUFFIX {                                                                    \
+  using C = P::cpx;                                                                            \
+  using SP = P::sp_t;                                                                          \
+  using TW = P::tw_t;                                                                          \
+  cudaError_t gather(void *dst, const Side &src, const EwArgs &e, cudaStream_t st) {           \
+    k_gather<C><<<ew_blocks(e.nlines * e.ldst), 256, 0, st>>>(                                \
+        (C *)dst, src, e.nlines, e.len, e.ldst, e.perm,                                        \
+        (const std::conditional<sizeof(C) == 16, double2, float4>::type *)e.chirp, e.cj,       \
+        (C *)e.x0s);                                                                           \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t spec_mul(void *y, const void *B, const EwArgs &e, cudaStream_t st) {             \
+    k_spec_mul<C, SP><<<ew_blocks(e.nlines * e.len), 256, 0, st>>>(                           \
+        (C *)y, (const SP *)B, e.nlines, e.len, (const C *)e.x0s, (C *)e.dc);                  \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t rader_scatter(const Side &dst, const void *y, const int *iperm, const EwArgs &e, \
+                            cudaStream_t st) {                                                 \
+    k_rader_scatter<C><<<ew_blocks(e.nlines * e.p), 256, 0, st>>>(                            \
+        dst, (const C *)y, e.nlines, e.p, e.len, e.off, iperm, (const C *)e.x0s,               \
+        (const C *)e.dc, e.cj, e.scale);                                                       \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t blue_unchirp(const Side &dst, const void *y, const EwArgs &e, cudaStream_t st) { \
+    k_blue_unchirp<C, SP><<<ew_blocks(e.nlines * e.p), 256, 0, st>>>(                         \
+        dst, (const C *)y, e.nlines, e.p, e.len, (const SP *)e.chirp, e.cj, e.scale);          \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t scatter(const Side &dst, const void *src, const EwArgs &e, cudaStream_t st) {    \
+    k_scatter<C><<<ew_blocks(e.nlines * e.len), 256, 0, st>>>(dst, (const C *)src, e.nlines,  \
+                                                              e.len, e.cj, e.scale);           \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t stage_tw(void *tw, const StageTab &t, long long total, cudaStream_t st) {        \
+    k_gen_stage_tw<TW><<<ew_blocks(total), 256, 0, st>>>((TW *)tw, t, total);                 \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t roots(void *tw, long long L, long long count, cudaStream_t st) {                 \
+    k_gen_roots<TW><<<ew_blocks(count), 256, 0, st>>>((TW *)tw, L, count);                    \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t spectrum(void *dst, const double2 *src, double s, long long n, cudaStream_t st) { \
+    k_store_spectrum<SP><<<ew_blocks(n), 256, 0, st>>>((SP *)dst, src, s, n);                 \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t untangle(const Side &dst, const void *Z, long long nl, int m, const void *tw,    \
+                       cudaStream_t st) {                                                      \
+    k_untangle<C, TW><<<ew_blocks(nl * (m / 2 + 1)), 256, 0, st>>>(dst, (const C *)Z, nl, m, \
+                                                                   (const TW *)tw);            \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t reverse_untangle(void *Z, const Side &src, long long nl, int m, int nb,          \
+                               const void *tw, cudaStream_t st) {                              \
+    k_reverse_untangle<C, TW><<<ew_blocks(nl * (m / 2 + 1)), 256, 0, st>>>(                   \
+        (C *)Z, src, nl, m, nb, (const TW *)tw);                                               \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t promote(void *dst, const Side &src, long long nl, int n, cudaStream_t st) {      \
+    k_promote<C><<<ew_blocks(nl * n), 256, 0, st>>>((C *)dst, src, nl, n);                    \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t copy_bins(const Side &dst, const void *src, long long nl, int n, cudaStream_t st) { \
+    k_copy_bins<C><<<ew_blocks(nl * (n / 2 + 1)), 256, 0, st>>>(dst, (const C *)src, nl, n);  \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t mirror(void *dst, const Side &src, long long nl, int n, int nb, cudaStream_t st) { \
+    k_mirror<C><<<ew_blocks(nl * n), 256, 0, st>>>((C *)dst, src, nl, n, nb);                 \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t take_real(const Side &dst, const void *src, long long nl, int n, double scale,   \
+                        cudaStream_t st) {                                                     \
+    k_take_real<C><<<ew_blocks(nl * n), 256, 0, st>>>(dst, (const C *)src, nl, n, scale);     \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  }                                                                                            \
+  }

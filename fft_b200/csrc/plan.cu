@@ -1,0 +1,832 @@
+// plan.cu -- line programs, 1-D executors and real executors.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+
+#include "plan.cuh"
+
+namespace gf {
+
+static thread_local std::string g_err;
+int set_err(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+const char *last_err() { return g_err.c_str(); }
+
+#define GF_CK(x)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess)                                                              \
+      return set_err(3, std::string(#x) + ": " + cudaGetErrorString(e_));               \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Integer helpers, restated from the reference router.
+// ---------------------------------------------------------------------------
+
+// plan.go:134-141
+bool smooth13(long long n) {
+  if (n < 1) return false;
+  for (long long p : {2, 3, 5, 7, 11, 13})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+// rader.go:232-245
+bool is_prime_ll(long long n) {
+  if (n < 2) return false;
+  if (n % 2 == 0) return n == 2;
+  for (long long d = 3; d * d <= n; d += 2)
+    if (n % d == 0) return false;
+  return true;
+}
+
+static long long modpow_h(long long b, long long e, long long m) {
+  long long r = 1;
+  b %= m;
+  while (e > 0) {
+    if (e & 1) r = (__int128)r * b % m;
+    e >>= 1;
+    b = (__int128)b * b % m;
+  }
+  return r;
+}
+
+// rader.go:178-212: smallest generator of (Z/pZ)*.
+long long primitive_root_ll(long long p) {
+  long long phi = p - 1, m = phi;
+  std::vector<long long> f;
+  for (long long d = 2; d * d <= m; d++)
+    if (m % d == 0) {
+      f.push_back(d);
+      while (m % d == 0) m /= d;
+    }
+  if (m > 1) f.push_back(m);
+  if (f.empty()) return 1;
+  for (long long g = 2;; g++) {
+    bool gen = true;
+    for (long long q : f)
+      if (modpow_h(g, phi / q, p) == 1) {
+        gen = false;
+        break;
+      }
+    if (gen) return g;
+  }
+}
+
+// plan.go:192-220
+bool conv_cost(long long m, double *cost) {
+  const double w2 = 2.0, w3 = 2.0, w5 = 2.8, w7 = 2.6;
+  double c = 0;
+  long long x = m;
+  while (x % 4 == 0) { c += w2; x /= 4; }
+  while (x % 2 == 0) { c += w2; x /= 2; }
+  while (x % 3 == 0) { c += w3; x /= 3; }
+  while (x % 5 == 0) { c += w5; x /= 5; }
+  while (x % 7 == 0) { c += w7; x /= 7; }
+  if (x != 1) return false;
+  if (cost) *cost = (double)m * c;
+  return true;
+}
+
+// plan.go:241-259
+long long best_conv_len(long long lo) {
+  if (lo < 1) lo = 1;
+  long long hi = lo + (lo * 4 + 9) / 10, best = lo;
+  double bc = 0;
+  bool have = false;
+  for (long long m = lo; m <= hi; m++) {
+    double c;
+    if (!conv_cost(m, &c)) continue;
+    if (!have || c < bc) { best = m; bc = c; have = true; }
+  }
+  return best;
+}
+
+// Radix schedule of a 13-smooth length for the Stockham stages: the power of
+// two is split into as few radix-16/8/4/2 stages as possible with the bits
+// spread evenly, then one stage per odd prime factor.
+std::vector<int> gpu_radices(long long n) {
+  std::vector<int> r;
+  long long m = n;
+  int a = 0;
+  while (m % 2 == 0) { a++; m /= 2; }
+  if (a > 0) {
+    int k = (a + 3) / 4;
+    for (int i = 0; i < k; i++) r.push_back(1 << (a / k + (i < a % k ? 1 : 0)));
+  }
+  for (int p : {3, 5, 7, 11, 13})
+    while (m % p == 0) { r.push_back(p); m /= p; }
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// Device properties and kernel lookup.
+// ---------------------------------------------------------------------------
+static int cur_device() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
+
+static size_t max_smem_optin() {
+  static std::mutex mu;
+  static std::map<int, size_t> cache;
+  int d = cur_device();
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(d);
+  if (it != cache.end()) return it->second;
+  int v = 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, d) != cudaSuccess || v <= 0)
+    v = 48 * 1024;
+  cache[d] = (size_t)v;
+  return (size_t)v;
+}
+
+static KFn kernel_for(int prec, int maxe, int op) {
+  switch (prec) {
+    case F64: return line_kernel_f64(maxe, op);
+    case F32: return line_kernel_f32(maxe, op);
+    default: return line_kernel_f32c(maxe, op);
+  }
+}
+
+static int ensure_smem(KFn f, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> done;
+  if (smem <= 48 * 1024) return 0;
+  auto key = std::make_pair(cur_device(), (const void *)f);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= smem) return 0;
+  GF_CK(cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  done[key] = smem;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// DevProg
+// ---------------------------------------------------------------------------
+DevProg::~DevProg() {
+  if (tw) cudaFree(tw);
+}
+
+static int pick_threads(long long n, int maxe, const std::vector<int> &rad) {
+  long long T = (n + maxe - 1) / maxe;
+  if (T < 1) T = 1;
+  for (; T <= 512; T++) {
+    bool ok = true;
+    for (int R : rad) {
+      const long long nb = n / R, per = (nb + T - 1) / T;
+      if (per > maxe / R) { ok = false; break; }
+    }
+    if (ok) return (int)T;
+  }
+  return -1;
+}
+
+static bool schedule_for(long long n, int prec, int &maxe, int &T, std::vector<int> &rad) {
+  if (n < 1 || !smooth13(n)) return false;
+  rad = gpu_radices(n);
+  if ((int)rad.size() > GF_MAXST) return false;
+  const size_t bytes = (size_t)spad_size((int)n) * csize(prec) + 2 * csize(prec);
+  if (bytes > max_smem_optin()) return false;
+  for (int me : {16, 32}) {
+    if (me == 32 && prec == F64) break;
+    const int t = pick_threads(n, me, rad);
+    if (t > 0) {
+      maxe = me;
+      T = t;
+      return true;
+    }
+  }
+  return false;
+}
+
+bool fits_single(long long n, int prec) {
+  int me, T;
+  std::vector<int> rad;
+  if (n <= 1) return true;
+  return schedule_for(n, prec, me, T, rad);
+}
+
+static int build_prog(long long n, int prec, std::shared_ptr<DevProg> &out) {
+  auto dp = std::make_shared<DevProg>();
+  dp->n = (int)n;
+  dp->prec = prec;
+  dp->device = cur_device();
+  LineProg &lp = dp->lp;
+  lp.n = (int)n;
+  if (n <= 1) {
+    lp.nst = 0;
+    lp.T = 1;
+    lp.maxe = 16;
+    dp->maxe = 16;
+    out = dp;
+    return 0;
+  }
+  int maxe = 16, T = 1;
+  std::vector<int> rad;
+  if (!schedule_for(n, prec, maxe, T, rad))
+    return set_err(5, "length " + std::to_string(n) + " has no single-CTA schedule");
+  lp.nst = (int)rad.size();
+  lp.T = T;
+  lp.maxe = maxe;
+  dp->maxe = maxe;
+  StageTab tab{};
+  tab.nst = lp.nst;
+  long long ns = 1, off = 0;
+  for (int s = 0; s < lp.nst; s++) {
+    lp.radix[s] = tab.radix[s] = rad[s];
+    lp.ns[s] = tab.ns[s] = (int)ns;
+    lp.twoff[s] = tab.twoff[s] = (int)off;
+    lp.nsdiv[s] = FastDiv((uint32_t)ns);
+    off += ns * (rad[s] - 1);
+    ns *= rad[s];
+  }
+  const long long total = off > 0 ? off : 1;
+  GF_CK(cudaMalloc(&dp->tw, total * twsize(prec)));
+  lp.tw = dp->tw;
+  cudaError_t e = cudaSuccess;
+  switch (prec) {
+    case F64: e = prec_f64::stage_tw(dp->tw, tab, off, 0); break;
+    case F32: e = prec_f32::stage_tw(dp->tw, tab, off, 0); break;
+    default: e = prec_f32c::stage_tw(dp->tw, tab, off, 0); break;
+  }
+  GF_CK(e);
+  GF_CK(cudaStreamSynchronize(0));
+  out = dp;
+  return 0;
+}
+
+template <class V>
+static std::shared_ptr<V> cache_get(std::map<std::tuple<int, long long, int>, std::shared_ptr<V>> &c,
+                                    std::mutex &mu, const std::tuple<int, long long, int> &k) {
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = c.find(k);
+  return it == c.end() ? nullptr : it->second;
+}
+
+std::shared_ptr<DevProg> get_prog(long long n, int prec) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, long long, int>, std::shared_ptr<DevProg>> cache;
+  auto key = std::make_tuple(cur_device(), n, prec);
+  if (auto p = cache_get(cache, mu, key)) return p;
+  std::shared_ptr<DevProg> p;
+  if (build_prog(n, prec, p) != 0) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;  // another thread won the race
+  cache[key] = p;
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+// Launch
+// ---------------------------------------------------------------------------
+static std::mutex g_lpc_mu;
+static std::map<std::tuple<int, long long, int, int>, int> g_lpc;
+void set_lpc_override(int prec, long long n, int op, int colmode, int lpc) {
+  std::lock_guard<std::mutex> lk(g_lpc_mu);
+  if (lpc <= 0) g_lpc.erase(std::make_tuple(prec, n, op, colmode));
+  else g_lpc[std::make_tuple(prec, n, op, colmode)] = lpc;
+}
+int get_lpc_override(int prec, long long n, int op, int colmode) {
+  std::lock_guard<std::mutex> lk(g_lpc_mu);
+  auto it = g_lpc.find(std::make_tuple(prec, n, op, colmode));
+  return it == g_lpc.end() ? 0 : it->second;
+}
+
+static int choose_lpc(const DevProg &dp, const KArgs &a, int op, long long nlines, bool conv) {
+  const int T = dp.lp.T;
+  const size_t line_bytes = (size_t)spad_size(dp.n) * csize(dp.prec) + (conv ? 2 * csize(dp.prec) : 0);
+  const size_t smax = max_smem_optin();
+  const int colmode = (a.in.stride != 1 || a.out.stride != 1) ? 1 : 0;
+  int lpc = get_lpc_override(dp.prec, dp.n, op, colmode);
+  if (lpc <= 0) {
+    lpc = std::max(1, 256 / T);
+    // keep two CTAs resident per SM where the lines allow it
+    while (lpc > 1 && (size_t)lpc * line_bytes > 100 * 1024) lpc--;
+    if (colmode) {
+      // columns: enough adjacent lines per CTA to fill 128-byte segments
+      const int want = dp.prec == F64 ? 8 : 16;
+      int cap = (int)std::min<size_t>(512 / T, smax / line_bytes);
+      lpc = std::max(lpc, std::min(want, cap));
+    }
+  }
+  lpc = std::min(lpc, std::max(1, 512 / T));
+  while (lpc > 1 && (size_t)lpc * line_bytes > smax) lpc--;
+  if (lpc > nlines) lpc = (int)std::max<long long>(1, nlines);
+  return lpc;
+}
+
+int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st, int lpc,
+                bool conv) {
+  if (nlines <= 0) return 0;
+  if (nlines >= (1ll << 31)) return set_err(5, "too many lines in one launch");
+  a.lp = dp.lp;
+  a.nlines = nlines;
+  if (lpc <= 0) lpc = choose_lpc(dp, a, op, nlines, conv);
+  a.lpc = lpc;
+  a.ndiv = FastDiv((uint32_t)dp.n);
+  a.lpcdiv = FastDiv((uint32_t)lpc);
+  const size_t smem = (size_t)lpc * spad_size(dp.n) * csize(dp.prec) + (conv ? 2 * lpc * csize(dp.prec) : 0);
+  KFn f = kernel_for(dp.prec, dp.maxe, op);
+  if (!f) return set_err(5, "no kernel instance for this precision/op");
+  if (int rc = ensure_smem(f, smem)) return rc;
+  const long long grid = (nlines + lpc - 1) / lpc;
+  f<<<(unsigned)grid, lpc * dp.lp.T, smem, st>>>(a);
+  GF_CK(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Exec1D
+// ---------------------------------------------------------------------------
+Exec1D::~Exec1D() {
+  for (void *p : {(void *)tw4, (void *)perm, (void *)iperm, (void *)jj, spec, chirp})
+    if (p) cudaFree(p);
+}
+
+size_t Exec1D::ws_bytes(long long nl) const {
+  const size_t c = csize(prec);
+  switch (kind) {
+    case K_FOURSTEP: return 3 * (size_t)n * nl * c + 256;
+    case K_RADER:
+      if (fused) return 0;
+      return (2 * (size_t)cl + 2) * nl * c + 256 + sub->ws_bytes(nl);
+    case K_BLUE:
+      if (fused) return 0;
+      return 2 * (size_t)m * nl * c + 256 + sub->ws_bytes(nl);
+    default: return 0;
+  }
+}
+
+static bool side_simple(const Side &s, long long &D) {
+  if (s.lpb.d == 1) { D = s.dist_b; return true; }
+  if (s.dist_b == (long long)s.lpb.d * s.dist_l) { D = s.dist_l; return true; }
+  return false;
+}
+
+static char *align256(char *p) { return (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255); }
+
+#define GF_PREC_CALL(prec, fn, ...)                                        \
+  ((prec) == F64 ? prec_f64::fn(__VA_ARGS__)                               \
+                 : ((prec) == F32 ? prec_f32::fn(__VA_ARGS__) : prec_f32c::fn(__VA_ARGS__)))
+
+int Exec1D::exec(const Side &in, const Side &out, long long nl, int cji, int cjo, double scale,
+                 void *ws, cudaStream_t st) const {
+  if (nl <= 0 || n == 0) return 0;
+  const size_t c = csize(prec);
+  switch (kind) {
+    case K_SINGLE: {
+      KArgs a{};
+      a.in = in;
+      a.out = out;
+      a.cj_in = cji;
+      a.cj_out = cjo;
+      a.scale = scale;
+      return launch_line(OP_C2C, *prog, a, nl, st);
+    }
+    case K_FOURSTEP: {
+      char *w = align256((char *)ws);
+      Side src = in;
+      long long Din = 0, Dout = 0;
+      if (!side_simple(in, Din)) {
+        EwArgs e{};
+        e.nlines = nl;
+        e.len = (int)n;
+        e.ldst = (int)n;
+        GF_CK(GF_PREC_CALL(prec, gather, w, in, e, st));
+        src = contig(w, n);
+        Din = n;
+        w += (size_t)n * nl * c;
+      }
+      char *ws1 = w;
+      w += (size_t)n * nl * c;
+      // pass 1: n2 columns of length n1, twiddled by W_n^{n2 k1}
+      KArgs a1{};
+      a1.in = mk_side(src.ptr, Din, src.stride, n2 * src.stride, n2);
+      a1.out = mk_side(ws1, n, 1, n2, n2);
+      a1.cj_in = cji;
+      a1.scale = 1.0;
+      a1.aux0 = tw4;
+      a1.ia = n;
+      if (int rc = launch_line(OP_C2C_TW, *p1, a1, nl * n2, st)) return rc;
+      // pass 2: n1 rows of length n2, written transposed
+      KArgs a2{};
+      a2.in = mk_side(ws1, n, n2, 1, n1);
+      a2.cj_out = cjo;
+      a2.scale = scale;
+      const bool direct = side_simple(out, Dout);
+      char *ws2 = w;
+      if (direct) a2.out = mk_side(out.ptr, Dout, out.stride, n1 * out.stride, n1);
+      else a2.out = mk_side(ws2, n, 1, n1, n1);
+      if (int rc = launch_line(OP_C2C, *p2, a2, nl * n1, st)) return rc;
+      if (!direct) {
+        EwArgs e{};
+        e.nlines = nl;
+        e.len = (int)n;
+        e.scale = 1.0;
+        GF_CK(GF_PREC_CALL(prec, scatter, out, ws2, e, st));
+      }
+      return 0;
+    }
+    case K_RADER: {
+      if (fused) {
+        KArgs a{};
+        a.in = in;
+        a.out = out;
+        a.cj_in = cji;
+        a.cj_out = cjo;
+        a.scale = scale;
+        a.aux0 = perm;
+        a.aux1 = iperm;
+        a.aux2 = spec;
+        a.ia = n;
+        a.ic = cyclic ? 0 : (int)(n - 1);
+        return launch_line(OP_RADER, *prog, a, nl, st, 0, true);
+      }
+      char *w = align256((char *)ws);
+      char *A = w;
+      char *B = A + (size_t)cl * nl * c;
+      char *x0s = B + (size_t)cl * nl * c;
+      char *dc = x0s + (size_t)nl * c;
+      char *wsub = align256(dc + (size_t)nl * c);
+      EwArgs e{};
+      e.nlines = nl;
+      e.len = (int)(n - 1);
+      e.ldst = (int)cl;
+      e.perm = perm;
+      e.cj = cji;
+      e.x0s = x0s;
+      GF_CK(GF_PREC_CALL(prec, gather, A, in, e, st));
+      if (int rc = sub->exec(contig(A, cl), contig(B, cl), nl, 0, 0, 1.0, wsub, st)) return rc;
+      EwArgs e2{};
+      e2.nlines = nl;
+      e2.len = (int)cl;
+      e2.x0s = x0s;
+      e2.dc = dc;
+      GF_CK(GF_PREC_CALL(prec, spec_mul, B, spec, e2, st));
+      if (int rc = sub->exec(contig(B, cl), contig(A, cl), nl, 0, 0, 1.0, wsub, st)) return rc;
+      EwArgs e3{};
+      e3.nlines = nl;
+      e3.p = (int)n;
+      e3.len = (int)cl;
+      e3.off = cyclic ? 0 : (int)(n - 1);
+      e3.x0s = x0s;
+      e3.dc = dc;
+      e3.cj = cjo;
+      e3.scale = scale;
+      GF_CK(GF_PREC_CALL(prec, rader_scatter, out, A, iperm, e3, st));
+      return 0;
+    }
+    case K_BLUE: {
+      if (fused) {
+        KArgs a{};
+        a.in = in;
+        a.out = out;
+        a.cj_in = cji;
+        a.cj_out = cjo;
+        a.scale = scale;
+        a.aux0 = chirp;
+        a.aux2 = spec;
+        a.ia = n;
+        return launch_line(OP_BLUE, *prog, a, nl, st, 0, true);
+      }
+      char *w = align256((char *)ws);
+      char *A = w;
+      char *B = A + (size_t)m * nl * c;
+      char *wsub = align256(B + (size_t)m * nl * c);
+      EwArgs e{};
+      e.nlines = nl;
+      e.len = (int)n;
+      e.ldst = (int)m;
+      e.chirp = chirp;
+      e.cj = cji;
+      GF_CK(GF_PREC_CALL(prec, gather, A, in, e, st));
+      if (int rc = sub->exec(contig(A, m), contig(B, m), nl, 0, 0, 1.0, wsub, st)) return rc;
+      EwArgs e2{};
+      e2.nlines = nl;
+      e2.len = (int)m;
+      GF_CK(GF_PREC_CALL(prec, spec_mul, B, spec, e2, st));
+      if (int rc = sub->exec(contig(B, m), contig(A, m), nl, 0, 0, 1.0, wsub, st)) return rc;
+      EwArgs e3{};
+      e3.nlines = nl;
+      e3.p = (int)n;
+      e3.len = (int)m;
+      e3.chirp = chirp;
+      e3.cj = cjo;
+      e3.scale = scale;
+      GF_CK(GF_PREC_CALL(prec, blue_unchirp, out, A, e3, st));
+      return 0;
+    }
+  }
+  return set_err(1, "bad executor kind");
+}
+
+std::string Exec1D::describe() const {
+  std::ostringstream o;
+  static const char *names[] = {"single", "fourstep", "rader", "bluestein"};
+  o << "{\"n\":" << n << ",\"engine\":\"" << names[kind] << "\"";
+  auto sched = [&](const DevProg &d) {
+    std::ostringstream s;
+    s << "{\"n\":" << d.n << ",\"T\":" << d.lp.T << ",\"maxe\":" << d.maxe << ",\"radices\":[";
+    for (int i = 0; i < d.lp.nst; i++) s << (i ? "," : "") << d.lp.radix[i];
+    s << "]}";
+    return s.str();
+  };
+  if (kind == K_SINGLE && prog) o << ",\"prog\":" << sched(*prog);
+  if (kind == K_FOURSTEP) o << ",\"n1\":" << n1 << ",\"n2\":" << n2 << ",\"p1\":" << sched(*p1) << ",\"p2\":" << sched(*p2);
+  if (kind == K_RADER) o << ",\"g\":" << g << ",\"cl\":" << cl << ",\"cyclic\":" << cyclic << ",\"fused\":" << (fused ? 1 : 0);
+  if (kind == K_BLUE) o << ",\"m\":" << m << ",\"fused\":" << (fused ? 1 : 0);
+  if ((kind == K_RADER || kind == K_BLUE) && fused && prog) o << ",\"prog\":" << sched(*prog);
+  if ((kind == K_RADER || kind == K_BLUE) && !fused && sub) o << ",\"conv\":" << sub->describe();
+  o << "}";
+  return o.str();
+}
+
+// FP64 spectrum of a convolution kernel b (length L, device FP64), scaled by
+// 1/L and stored in the precision's spectrum form.
+static int make_spectrum(int prec, double2 *b, long long L, void **spec_out) {
+  auto ex = get_exec(L, F64);
+  if (!ex) return 3;
+  double2 *B = nullptr;
+  void *ws = nullptr;
+  GF_CK(cudaMalloc(&B, L * sizeof(double2)));
+  size_t wsb = ex->ws_bytes(1);
+  if (wsb) GF_CK(cudaMalloc(&ws, wsb));
+  int rc = ex->exec(contig(b, L), contig(B, L), 1, 0, 0, 1.0, ws, 0);
+  if (rc == 0) {
+    cudaError_t e = cudaMalloc(spec_out, L * spsize(prec));
+    if (e == cudaSuccess) e = GF_PREC_CALL(prec, spectrum, *spec_out, B, 1.0 / (double)L, L, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) rc = set_err(3, std::string("spectrum: ") + cudaGetErrorString(e));
+  }
+  cudaFree(B);
+  if (ws) cudaFree(ws);
+  return rc;
+}
+
+static int build_exec(long long n, int prec, std::shared_ptr<Exec1D> &out) {
+  auto ex = std::make_shared<Exec1D>();
+  ex->n = n;
+  ex->prec = prec;
+  ex->device = cur_device();
+  if (n < 0) return set_err(1, "negative length");
+  if (n <= 1 || fits_single(n, prec)) {
+    ex->kind = K_SINGLE;
+    ex->prog = get_prog(n, prec);
+    if (!ex->prog) return 3;
+    out = ex;
+    return 0;
+  }
+  if (smooth13(n)) {
+    // four-step: n = n1 * n2 with both single-CTA lengths, n1 closest to sqrt
+    long long best = 0;
+    double bd = 1e300;
+    for (long long d = 2; d * d <= n * 4 && d < n; d++) {
+      if (n % d) continue;
+      if (!fits_single(d, prec) || !fits_single(n / d, prec)) continue;
+      const double dist = std::fabs(std::log((double)d) - 0.5 * std::log((double)n));
+      if (dist < bd) { bd = dist; best = d; }
+    }
+    if (!best) return set_err(5, "length " + std::to_string(n) + " too long for a two-pass split");
+    ex->kind = K_FOURSTEP;
+    ex->n1 = best;
+    ex->n2 = n / best;
+    ex->p1 = get_prog(ex->n1, prec);
+    ex->p2 = get_prog(ex->n2, prec);
+    if (!ex->p1 || !ex->p2) return 3;
+    GF_CK(cudaMalloc(&ex->tw4, n * twsize(prec)));
+    GF_CK(GF_PREC_CALL(prec, roots, ex->tw4, n, n, 0));
+    GF_CK(cudaStreamSynchronize(0));
+    out = ex;
+    return 0;
+  }
+  if (n >= 700 && is_prime_ll(n)) {
+    // Rader (rader.go:51-91)
+    ex->kind = K_RADER;
+    const long long q = n - 1;
+    ex->g = primitive_root_ll(n);
+    ex->cyclic = smooth13(q) ? 1 : 0;
+    ex->cl = ex->cyclic ? q : best_conv_len(2 * q);
+    GF_CK(cudaMalloc(&ex->perm, q * sizeof(int)));
+    GF_CK(cudaMalloc(&ex->iperm, q * sizeof(int)));
+    GF_CK(gen_rader_perm(ex->perm, ex->iperm, n, ex->g, 0));
+    double2 *b = nullptr;
+    GF_CK(cudaMalloc(&b, ex->cl * sizeof(double2)));
+    GF_CK(gen_rader_kernel(b, ex->perm, n, ex->cl, ex->cyclic, 0));
+    int rc = make_spectrum(prec, b, ex->cl, &ex->spec);
+    cudaFree(b);
+    if (rc) return rc;
+    auto conv = get_exec(ex->cl, prec);
+    if (!conv) return 3;
+    if (conv->kind == K_SINGLE) {
+      ex->fused = true;
+      ex->prog = conv->prog;
+    } else {
+      ex->sub = conv;
+    }
+    out = ex;
+    return 0;
+  }
+  // Bluestein (bluestein.go:28-48)
+  ex->kind = K_BLUE;
+  long long m = 1;
+  while (m < 2 * n - 1) m <<= 1;
+  ex->m = m;
+  double2 *w = nullptr, *b = nullptr;
+  GF_CK(cudaMalloc(&ex->jj, n * sizeof(long long)));
+  GF_CK(cudaMalloc(&w, n * sizeof(double2)));
+  GF_CK(cudaMalloc(&b, m * sizeof(double2)));
+  GF_CK(gen_chirp(ex->jj, w, n, 0));
+  GF_CK(gen_blue_kernel(b, w, n, m, 0));
+  int rc = make_spectrum(prec, b, m, &ex->spec);
+  if (rc == 0) {
+    cudaError_t e = cudaMalloc(&ex->chirp, n * spsize(prec));
+    if (e == cudaSuccess) e = GF_PREC_CALL(prec, spectrum, ex->chirp, w, 1.0, n, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) rc = set_err(3, std::string("chirp: ") + cudaGetErrorString(e));
+  }
+  cudaFree(w);
+  cudaFree(b);
+  if (rc) return rc;
+  auto conv = get_exec(m, prec);
+  if (!conv) return 3;
+  if (conv->kind == K_SINGLE) {
+    ex->fused = true;
+    ex->prog = conv->prog;
+  } else {
+    ex->sub = conv;
+  }
+  out = ex;
+  return 0;
+}
+
+std::shared_ptr<const Exec1D> get_exec(long long n, int prec) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, long long, int>, std::shared_ptr<Exec1D>> cache;
+  auto key = std::make_tuple(cur_device(), n, prec);
+  if (auto p = cache_get(cache, mu, key)) return p;
+  // built outside the lock: prime lengths re-enter get_exec for their
+  // convolution (the reference's cachedPlan does the same, plan.go:295-300)
+  std::shared_ptr<Exec1D> p;
+  if (build_exec(n, prec, p) != 0) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  cache[key] = p;
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+// ExecReal
+// ---------------------------------------------------------------------------
+ExecReal::~ExecReal() {
+  if (tw2) cudaFree(tw2);
+}
+
+size_t ExecReal::ws_bytes(long long nl) const {
+  const size_t c = csize(prec);
+  switch (mode) {
+    case R_PACKED_MULTI: return (size_t)(n / 2) * nl * c + 256 + cx->ws_bytes(nl);
+    case R_FULL_MULTI: return 2 * (size_t)n * nl * c + 256 + cx->ws_bytes(nl);
+    default: return 0;
+  }
+}
+
+int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaStream_t st) const {
+  if (nl <= 0 || n == 0) return 0;
+  const size_t c = csize(prec);
+  const long long m = n / 2;
+  switch (mode) {
+    case R_PACKED_FUSED: {
+      KArgs a{};
+      a.in = in;
+      a.out = out;
+      a.aux0 = tw2;
+      a.scale = 1.0;
+      return launch_line(OP_R2C, *cx->prog, a, nl, st);
+    }
+    case R_FULL_FUSED: {
+      KArgs a{};
+      a.in = in;
+      a.out = out;
+      a.scale = 1.0;
+      return launch_line(OP_R2C_FULL, *cx->prog, a, nl, st);
+    }
+    case R_PACKED_MULTI: {
+      if (in.stride != 1 || (in.dist_b % 2) || (in.dist_l % 2))
+        return set_err(5, "packed real transform needs unit-stride rows with even distances");
+      char *Z = align256((char *)ws);
+      char *wsub = align256(Z + (size_t)m * nl * c);
+      Side zin = mk_side(in.ptr, in.dist_b / 2, in.dist_l / 2, 1, in.lpb.d);
+      if (int rc = cx->exec(zin, contig(Z, m), nl, 0, 0, 1.0, wsub, st)) return rc;
+      GF_CK(GF_PREC_CALL(prec, untangle, out, Z, nl, (int)m, tw2, st));
+      return 0;
+    }
+    case R_FULL_MULTI: {
+      char *A = align256((char *)ws);
+      char *B = A + (size_t)n * nl * c;
+      char *wsub = align256(B + (size_t)n * nl * c);
+      GF_CK(GF_PREC_CALL(prec, promote, A, in, nl, (int)n, st));
+      if (int rc = cx->exec(contig(A, n), contig(B, n), nl, 0, 0, 1.0, wsub, st)) return rc;
+      GF_CK(GF_PREC_CALL(prec, copy_bins, out, B, nl, (int)n, st));
+      return 0;
+    }
+  }
+  return set_err(1, "bad real mode");
+}
+
+int ExecReal::c2r(const Side &in, int nb, const Side &out, long long nl, double scale, void *ws,
+                  cudaStream_t st) const {
+  if (nl <= 0 || n == 0) return 0;
+  const size_t c = csize(prec);
+  const long long m = n / 2;
+  switch (mode) {
+    case R_PACKED_FUSED: {
+      KArgs a{};
+      a.in = in;
+      a.out = out;
+      a.aux0 = tw2;
+      a.ic = nb;
+      a.scale = scale / (double)m;
+      return launch_line(OP_C2R, *cx->prog, a, nl, st);
+    }
+    case R_FULL_FUSED: {
+      KArgs a{};
+      a.in = in;
+      a.out = out;
+      a.ic = nb;
+      a.scale = scale / (double)n;
+      return launch_line(OP_C2R_FULL, *cx->prog, a, nl, st);
+    }
+    case R_PACKED_MULTI: {
+      if (out.stride != 1 || (out.dist_b % 2) || (out.dist_l % 2))
+        return set_err(5, "packed real transform needs unit-stride rows with even distances");
+      char *Z = align256((char *)ws);
+      char *wsub = align256(Z + (size_t)m * nl * c);
+      GF_CK(GF_PREC_CALL(prec, reverse_untangle, Z, in, nl, (int)m, nb, tw2, st));
+      Side zout = mk_side(out.ptr, out.dist_b / 2, out.dist_l / 2, 1, out.lpb.d);
+      return cx->exec(contig(Z, m), zout, nl, 0, 1, scale / (double)m, wsub, st);
+    }
+    case R_FULL_MULTI: {
+      char *A = align256((char *)ws);
+      char *B = A + (size_t)n * nl * c;
+      char *wsub = align256(B + (size_t)n * nl * c);
+      GF_CK(GF_PREC_CALL(prec, mirror, A, in, nl, (int)n, nb, st));
+      if (int rc = cx->exec(contig(A, n), contig(B, n), nl, 0, 0, 1.0, wsub, st)) return rc;
+      GF_CK(GF_PREC_CALL(prec, take_real, out, B, nl, (int)n, scale / (double)n, st));
+      return 0;
+    }
+  }
+  return set_err(1, "bad real mode");
+}
+
+std::string ExecReal::describe() const {
+  static const char *names[] = {"packed_fused", "packed_multi", "full_fused", "full_multi"};
+  std::ostringstream o;
+  o << "{\"n\":" << n << ",\"mode\":\"" << names[mode] << "\",\"complex\":" << cx->describe() << "}";
+  return o.str();
+}
+
+static int build_real(long long n, int prec, std::shared_ptr<ExecReal> &out) {
+  auto r = std::make_shared<ExecReal>();
+  r->n = n;
+  r->prec = prec;
+  r->device = cur_device();
+  if (n >= 2 && n % 2 == 0) {
+    const long long m = n / 2;
+    r->cx = get_exec(m, prec);
+    if (!r->cx) return 3;
+    r->mode = r->cx->kind == K_SINGLE ? R_PACKED_FUSED : R_PACKED_MULTI;
+    GF_CK(cudaMalloc(&r->tw2, (m + 1) * twsize(prec)));
+    GF_CK(GF_PREC_CALL(prec, roots, r->tw2, n, m + 1, 0));
+    GF_CK(cudaStreamSynchronize(0));
+  } else {
+    r->cx = get_exec(n, prec);
+    if (!r->cx) return 3;
+    r->mode = r->cx->kind == K_SINGLE ? R_FULL_FUSED : R_FULL_MULTI;
+  }
+  out = r;
+  return 0;
+}
+
+std::shared_ptr<const ExecReal> get_real(long long n, int prec) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, long long, int>, std::shared_ptr<ExecReal>> cache;
+  auto key = std::make_tuple(cur_device(), n, prec);
+  if (auto p = cache_get(cache, mu, key)) return p;
+  std::shared_ptr<ExecReal> p;
+  if (build_real(n, prec, p) != 0) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  cache[key] = p;
+  return p;
+}
+
+}  // namespace gf

@@ -1,0 +1,121 @@
+// plan.cuh -- host-side plan objects of the B200 FFT engine.
+//
+//   DevProg   one single-CTA line program (length n, precision): radix
+//             schedule, threads per line, device twiddle planes.
+//   Exec1D    a batched, strided 1-D complex transform of any length: one
+//             fused launch (smooth lengths that fit one CTA, and Rader /
+//             Bluestein whose convolution fits one CTA), a two-pass four-step
+//             split, or a multi-pass convolution over a workspace.
+//   ExecReal  the real forward/inverse of one length (packed half-length
+//             transform for even n, full complex line for odd n).
+//
+// Routing follows the reference router (plan.go:42-73): powers of two and
+// 13-smooth lengths are Cooley-Tukey, primes >= 700 are Rader (cyclic at
+// p-1 when p-1 is 13-smooth, else padded-linear at bestConvLen(2(p-1))), and
+// every other length is Bluestein at the next power of two >= 2n-1.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "dispatch.h"
+
+namespace gf {
+
+int set_err(int code, const std::string &msg);
+const char *last_err();
+
+inline size_t csize(int prec) { return prec == F64 ? 16 : 8; }
+inline size_t rsize(int prec) { return prec == F64 ? 8 : 4; }
+inline size_t twsize(int prec) { return prec == F32 ? 8 : 16; }
+inline size_t spsize(int) { return 16; }
+
+// integer routing helpers (plan.go, rader.go)
+bool smooth13(long long n);
+bool is_prime_ll(long long n);
+long long primitive_root_ll(long long p);
+bool conv_cost(long long m, double *cost);
+long long best_conv_len(long long lo);
+std::vector<int> gpu_radices(long long n);
+
+struct DevProg {
+  int n = 0, prec = 0, maxe = 16, device = 0;
+  LineProg lp{};
+  void *tw = nullptr;
+  ~DevProg();
+};
+
+enum ExecKind { K_SINGLE = 0, K_FOURSTEP = 1, K_RADER = 2, K_BLUE = 3 };
+
+struct Exec1D {
+  long long n = 0;
+  int prec = 0, kind = K_SINGLE, device = 0;
+  std::shared_ptr<DevProg> prog;        // SINGLE: length n; fused conv: length cl / m
+  std::shared_ptr<DevProg> p1, p2;      // FOURSTEP: lengths n1, n2
+  std::shared_ptr<const Exec1D> sub;    // multi-pass convolution at cl / m
+  long long n1 = 0, n2 = 0;
+  void *tw4 = nullptr;                  // FOURSTEP: W_n^e, e < n
+  bool fused = false;
+  long long cl = 0, g = 0, m = 0;
+  int cyclic = 0;
+  int *perm = nullptr, *iperm = nullptr;
+  long long *jj = nullptr;
+  void *spec = nullptr, *chirp = nullptr;
+  ~Exec1D();
+  size_t ws_bytes(long long nlines) const;
+  int exec(const Side &in, const Side &out, long long nlines, int cj_in, int cj_out, double scale,
+           void *ws, cudaStream_t st) const;
+  std::string describe() const;
+};
+
+enum RealMode { R_PACKED_FUSED = 0, R_PACKED_MULTI = 1, R_FULL_FUSED = 2, R_FULL_MULTI = 3 };
+
+struct ExecReal {
+  long long n = 0;
+  int prec = 0, mode = R_FULL_FUSED, device = 0;
+  std::shared_ptr<const Exec1D> cx;  // half (even) or full (odd) complex exec
+  void *tw2 = nullptr;               // W_n^k, k = 0..n/2 (packed modes)
+  ~ExecReal();
+  size_t ws_bytes(long long nlines) const;
+  // in: reals, out: bins
+  int r2c(const Side &in, const Side &out, long long nlines, void *ws, cudaStream_t st) const;
+  // in: bins (nb available per line), out: reals; the result is the
+  // reference-normalised inverse (1/n) times `scale`.
+  int c2r(const Side &in, int nb, const Side &out, long long nlines, double scale, void *ws,
+          cudaStream_t st) const;
+  std::string describe() const;
+};
+
+// Cached constructors (per device, length, precision); nullptr + error set on
+// failure.
+std::shared_ptr<DevProg> get_prog(long long n, int prec);
+std::shared_ptr<const Exec1D> get_exec(long long n, int prec);
+std::shared_ptr<const ExecReal> get_real(long long n, int prec);
+bool fits_single(long long n, int prec);
+
+// Launch helper for the line kernels.
+int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st,
+                int lpc = 0, bool conv = false);
+
+inline Side mk_side(void *p, long long dist_b, long long dist_l, long long stride, long long lpb) {
+  Side s;
+  s.ptr = p;
+  s.dist_b = dist_b;
+  s.dist_l = dist_l;
+  s.stride = stride;
+  s.lpb = FastDiv((uint32_t)(lpb < 1 ? 1 : lpb));
+  return s;
+}
+// Contiguous lines of length len.
+inline Side contig(void *p, long long len) { return mk_side(p, len, 0, 1, 1); }
+
+// Autotuned lines-per-CTA overrides (key: prec, n, op, column-mode).
+void set_lpc_override(int prec, long long n, int op, int colmode, int lpc);
+int get_lpc_override(int prec, long long n, int op, int colmode);
+
+}  // namespace gf

@@ -1,0 +1,145 @@
+"""Device-resident plans on torch tensors (plumbing only: torch owns the
+memory and the stream; every transform runs in libgofft_b200.so).
+
+    p = DevicePlan("c2c", "f64", [1024], batch=256)
+    y = p.c2c(x)                    # x: complex128 cuda tensor (256, 1024)
+    X = DevicePlan("r2c", "f32mixed", [512, 512], batch=32).r2c(img)
+"""
+import ctypes
+import json
+
+import torch
+
+from ._lib import GOFFT_C2C, GOFFT_F32, GOFFT_F32MIXED, GOFFT_F64, GOFFT_R2C, check, lib
+
+PRECISIONS = {"f64": GOFFT_F64, "f32": GOFFT_F32, "f32mixed": GOFFT_F32MIXED}
+KINDS = {"c2c": GOFFT_C2C, "r2c": GOFFT_R2C}
+CDT = {GOFFT_F64: torch.complex128, GOFFT_F32: torch.complex64, GOFFT_F32MIXED: torch.complex64}
+RDT = {GOFFT_F64: torch.float64, GOFFT_F32: torch.float32, GOFFT_F32MIXED: torch.float32}
+
+
+def _stream(stream):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _need(t, dtype, what):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("%s must be a CUDA tensor" % what)
+    if t.dtype != dtype:
+        raise TypeError("%s must be %s, got %s" % (what, dtype, t.dtype))
+    if not t.is_contiguous():
+        raise ValueError("%s must be contiguous" % what)
+
+
+class DevicePlan:
+    """A batched plan on the current CUDA device (gofft_plan_create)."""
+
+    def __init__(self, kind, precision, shape, batch=1, istride=0, idist=0, ostride=0, odist=0):
+        self.kind = KINDS[kind] if isinstance(kind, str) else int(kind)
+        self.prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        self.shape = [int(s) for s in shape]
+        self.batch = int(batch)
+        sh = (ctypes.c_int64 * len(self.shape))(*self.shape)
+        h = ctypes.c_void_p()
+        check(lib().gofft_plan_create(self.kind, self.prec, sh, len(self.shape), self.batch, istride, idist,
+                                      ostride, odist, ctypes.byref(h)))
+        self._h = h
+        self.cdtype = CDT[self.prec]
+        self.rdtype = RDT[self.prec]
+        n = 1
+        for s in self.shape:
+            n *= s
+        self.numel = n
+        self.bins = n // self.shape[-1] * (self.shape[-1] // 2 + 1)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def c2c(self, x, out=None, inverse=False, stream=None):
+        _need(x, self.cdtype, "x")
+        if out is None:
+            out = torch.empty_like(x)
+        _need(out, self.cdtype, "out")
+        check(lib().gofft_exec_c2c(self._h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                   1 if inverse else 0, _stream(stream)))
+        return out
+
+    def r2c(self, x, out=None, stream=None):
+        _need(x, self.rdtype, "x")
+        if out is None:
+            out = torch.empty((self.batch, self.bins), dtype=self.cdtype, device=x.device)
+        _need(out, self.cdtype, "out")
+        check(lib().gofft_exec_r2c(self._h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                   _stream(stream)))
+        return out
+
+    def c2r(self, X, out=None, nbins=0, stream=None):
+        _need(X, self.cdtype, "X")
+        if out is None:
+            out = torch.empty((self.batch, self.numel), dtype=self.rdtype, device=X.device)
+        _need(out, self.rdtype, "out")
+        check(lib().gofft_exec_c2r(self._h, ctypes.c_void_p(X.data_ptr()), int(nbins),
+                                   ctypes.c_void_p(out.data_ptr()), _stream(stream)))
+        return out
+
+    # host-pointer variants (copies inside the call): numpy or pinned tensors
+    def c2c_host(self, x_ptr, out_ptr, inverse=False):
+        check(lib().gofft_exec_c2c_host(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(out_ptr),
+                                        1 if inverse else 0))
+
+    def r2c_host(self, x_ptr, out_ptr):
+        check(lib().gofft_exec_r2c_host(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(out_ptr)))
+
+    def c2r_host(self, x_ptr, out_ptr, nbins=0):
+        check(lib().gofft_exec_c2r_host(self._h, ctypes.c_void_p(x_ptr), int(nbins), ctypes.c_void_p(out_ptr)))
+
+    def describe(self):
+        n = lib().gofft_plan_describe(self._h, None, 0)
+        buf = ctypes.create_string_buffer(int(n) + 1)
+        lib().gofft_plan_describe(self._h, buf, n + 1)
+        return json.loads(buf.value.decode())
+
+    def table(self, which):
+        n = lib().gofft_plan_table(self._h, int(which), None, 0)
+        if n < 0:
+            return None
+        out = (ctypes.c_int64 * max(1, n))()
+        lib().gofft_plan_table(self._h, int(which), out, n)
+        return list(out[:n])
+
+    def workspace_bytes(self):
+        v = ctypes.c_size_t()
+        check(lib().gofft_plan_workspace_size(self._h, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if self._h:
+            lib().gofft_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def spectrogram(x, segment, overlap, window, d, precision="f64", stream=None):
+    """Fused spectrogram (freq.go:107-127) of a device signal; returns a
+    (frames, segment//2+1) tensor of one-sided densities."""
+    prec = PRECISIONS[precision]
+    _need(x, RDT[prec], "x")
+    _need(window, RDT[prec], "window")
+    nf = ctypes.c_int64()
+    check(lib().gofft_spectrogram_device(prec, ctypes.c_void_p(x.data_ptr()), x.numel(), int(segment),
+                                         int(overlap), ctypes.c_void_p(window.data_ptr()), float(d), None,
+                                         ctypes.byref(nf), _stream(stream)))
+    out = torch.empty((nf.value, int(segment) // 2 + 1), dtype=RDT[prec], device=x.device)
+    if nf.value:
+        check(lib().gofft_spectrogram_device(prec, ctypes.c_void_p(x.data_ptr()), x.numel(), int(segment),
+                                             int(overlap), ctypes.c_void_p(window.data_ptr()), float(d),
+                                             ctypes.c_void_p(out.data_ptr()), ctypes.byref(nf),
+                                             _stream(stream)))
+    return out

@@ -1,0 +1,182 @@
+/*
+ * gofft.h -- C-ABI of the B200 FFT engine (libgofft_b200.so).
+ *
+ * The engine is a drop-in for the transform path of go-fft/fft.  Two layers:
+ *
+ *  1. The reference-facing entry points (gofft_new_plan ... gofft_spectrogram)
+ *     mirror the Go API one call for one call: host buffers of complex128
+ *     (interleaved re,im doubles) or float64, one transform per call, the same
+ *     argument meaning and normalisation.  A cgo binding calls these (see
+ *     INTEGRATION.md).  Argument errors that the Go API turns into a panic
+ *     return GOFFT_EINVAL with the reference's panic text in
+ *     gofft_last_error().
+ *
+ *  2. Device-resident plans (gofft_plan_create / gofft_exec_*) for batched,
+ *     strided transforms on device pointers in FP64 or the FP32 forms, plus
+ *     host-pointer variants that copy in and out inside the call.
+ *
+ * Every function returns a gofft_status; none aborts.  Plans are immutable
+ * after creation.  A plan's workspace is shared by its executions, so
+ * executions of one plan must not overlap on the device; the host-pointer and
+ * reference-facing entry points serialise on a per-plan lock.
+ */
+#ifndef GOFFT_H
+#define GOFFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GOFFT_API __attribute__((visibility("default")))
+#else
+#define GOFFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gofft_plan gofft_plan;
+typedef void *gofft_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+typedef enum {
+  GOFFT_OK = 0,
+  GOFFT_EINVAL = 1,       /* invalid argument (reference: panic) */
+  GOFFT_ENOMEM = 2,       /* device allocation failed */
+  GOFFT_ECUDA = 3,        /* CUDA runtime error */
+  GOFFT_ETIMEOUT = 4,     /* a bounded device wait expired */
+  GOFFT_EUNSUPPORTED = 5  /* shape/layout not supported by this build */
+} gofft_status;
+
+typedef enum {
+  GOFFT_C2C = 0, /* complex <-> complex */
+  GOFFT_R2C = 1  /* real forward (R2C) and its inverse (C2R); last axis real */
+} gofft_kind;
+
+typedef enum {
+  GOFFT_F64 = 0,      /* complex128 / float64: the parity form */
+  GOFFT_F32 = 1,      /* complex64, FP64-generated twiddles rounded to FP32 */
+  GOFFT_F32MIXED = 2  /* complex64, FP64 twiddles as hi+lo FP32 pairs */
+} gofft_precision;
+
+/* Last error message of the calling thread ("" if none). */
+GOFFT_API const char *gofft_last_error(void);
+/* Library version string. */
+GOFFT_API const char *gofft_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* 1. Reference-facing entry points (FP64, host buffers, one call each).     */
+/* ------------------------------------------------------------------------ */
+
+/* NewPlan (plan.go:42-73): a plan for length n >= 0; serves FFT and IFFT. */
+GOFFT_API int gofft_new_plan(int64_t n, gofft_plan **out);
+/* cachedPlan (plan.go:301-317): the shared memoised plan for n (not owned by
+ * the caller; never destroy it). */
+GOFFT_API int gofft_cached_plan(int64_t n, gofft_plan **out);
+/* Plan.Len (plan.go:86). */
+GOFFT_API int64_t gofft_plan_len(const gofft_plan *p);
+/* Plan.FFT (plan.go:91-94): dst, src hold Len() complex128; dst may alias. */
+GOFFT_API int gofft_plan_fft(gofft_plan *p, double *dst, const double *src);
+/* Plan.IFFT (plan.go:98-109): inverse normalised by 1/N; dst may alias. */
+GOFFT_API int gofft_plan_ifft(gofft_plan *p, double *dst, const double *src);
+
+/* NewRealPlan (realplan.go:37-58). */
+GOFFT_API int gofft_new_real_plan(int64_t n, gofft_plan **out);
+/* RealPlan.RFFT (realplan.go:77-116): src n float64 -> dst n/2+1 complex128. */
+GOFFT_API int gofft_real_plan_rfft(gofft_plan *p, double *dst, const double *src);
+/* RealPlan.IRFFT (realplan.go:181-192): reads min(nsrc, n/2+1) bins (missing
+ * bins are zero, imaginary parts of DC/Nyquist ignored); writes n float64
+ * normalised by 1/n. */
+GOFFT_API int gofft_real_plan_irfft(gofft_plan *p, double *dst, const double *src, int64_t nsrc);
+
+/* FFT / IFFT / FFTReal (fft.go:14-51): out has n complex128. */
+GOFFT_API int gofft_fft(const double *x, int64_t n, double *out);
+GOFFT_API int gofft_ifft(const double *x, int64_t n, double *out);
+GOFFT_API int gofft_fft_real(const double *x, int64_t n, double *out);
+/* RFFT (rfft.go:19-26): out has n/2+1 complex128 (0 for n == 0). */
+GOFFT_API int gofft_rfft(const double *x, int64_t n, double *out);
+/* IRFFT (rfft.go:39-45): spectrum of nspec bins -> n float64 (n <= 0: none). */
+GOFFT_API int gofft_irfft(const double *spectrum, int64_t nspec, int64_t n, double *out);
+
+/* FFTN / IFFTN (ndfft.go:22-33): data of len complex128, row-major shape of
+ * rank dims (rank 0 = scalar).  EINVAL ("fft: shape lengths must be
+ * positive" / "fft: shape product does not match len(data)") where the
+ * reference panics.  out has len complex128. */
+GOFFT_API int gofft_fftn(const double *data, int64_t len, const int64_t *shape, int rank, double *out);
+GOFFT_API int gofft_ifftn(const double *data, int64_t len, const int64_t *shape, int rank, double *out);
+/* FFT2 / IFFT2 (ndfft.go:37-45). */
+GOFFT_API int gofft_fft2(const double *data, int64_t len, int64_t rows, int64_t cols, double *out);
+GOFFT_API int gofft_ifft2(const double *data, int64_t len, int64_t rows, int64_t cols, double *out);
+/* RFFT2 (rfft2.go:22-74): rows*cols float64 -> rows*(cols/2+1) complex128. */
+GOFFT_API int gofft_rfft2(const double *data, int64_t len, int64_t rows, int64_t cols, double *out);
+/* IRFFT2 (rfft2.go:87-138): reads up to rows*(cols/2+1) bins of len (the rest
+ * zero) -> rows*cols float64 normalised by 1/(rows*cols). */
+GOFFT_API int gofft_irfft2(const double *data, int64_t len, int64_t rows, int64_t cols, double *out);
+
+/* Hann (window.go:20-22): symmetric window of length n (n <= 0: none). */
+GOFFT_API int gofft_hann(int64_t n, double *out);
+/* PSD (freq.go:69-90): one-sided density of n reals at spacing d -> n/2+1. */
+GOFFT_API int gofft_psd(const double *x, int64_t n, double d, double *out);
+/* Spectrogram (freq.go:107-127): frames of `segment` samples every
+ * segment-overlap samples, windowed, PSD each.  *nframes receives the frame
+ * count; out (frames*(segment/2+1) float64) may be NULL to query it. */
+GOFFT_API int gofft_spectrogram(const double *x, int64_t nx, int64_t segment, int64_t overlap,
+                      const double *window, int64_t nwindow, double d, double *out,
+                      int64_t *nframes);
+
+/* ------------------------------------------------------------------------ */
+/* 2. Device-resident plans.                                                 */
+/* ------------------------------------------------------------------------ */
+
+/* Plan for `batch` transforms of a row-major `shape` (rank >= 1).
+ *  C2C: element i (flattened index) of transform b is at b*idist + i*istride
+ *       (rank 1 any strides; rank > 1 requires istride == ostride == 1).
+ *  R2C: the last axis is real of length shape[rank-1] = n; the complex side
+ *       has n/2+1 bins on that axis.  "in" is the real side for strides and
+ *       distances (idist/istride in reals, odist/ostride in complex bins);
+ *       rank is 1 or 2.
+ * Strides/distances of 0 select the contiguous defaults. */
+GOFFT_API int gofft_plan_create(int kind, int precision, const int64_t *shape, int rank, int64_t batch,
+                      int64_t istride, int64_t idist, int64_t ostride, int64_t odist,
+                      gofft_plan **out);
+GOFFT_API int gofft_plan_destroy(gofft_plan *p);
+/* Bytes of device workspace the plan owns. */
+GOFFT_API int gofft_plan_workspace_size(const gofft_plan *p, size_t *bytes);
+/* JSON description of the plan (engine per axis, radix schedule, launch
+ * shape); returns the full length, writes at most cap bytes. */
+GOFFT_API int64_t gofft_plan_describe(const gofft_plan *p, char *buf, int64_t cap);
+
+/* Forward (inverse = 0) or normalised inverse (inverse = 1) C2C on device
+ * pointers.  in == out is allowed. */
+GOFFT_API int gofft_exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, gofft_stream stream);
+/* R2C on device pointers (real in, complex out). */
+GOFFT_API int gofft_exec_r2c(gofft_plan *p, const void *in, void *out, gofft_stream stream);
+/* C2R on device pointers: nbins complex bins per last-axis line are read
+ * (nbins <= 0 means n/2+1); output normalised by 1/prod(shape). */
+GOFFT_API int gofft_exec_c2r(gofft_plan *p, const void *in, int64_t nbins, void *out, gofft_stream stream);
+
+/* Host-pointer variants: copy host -> device, execute, copy back, synchronise.
+ * Pinned host memory makes the copies asynchronous DMA. */
+GOFFT_API int gofft_exec_c2c_host(gofft_plan *p, const void *in, void *out, int inverse);
+GOFFT_API int gofft_exec_r2c_host(gofft_plan *p, const void *in, void *out);
+GOFFT_API int gofft_exec_c2r_host(gofft_plan *p, const void *in, int64_t nbins, void *out);
+
+/* Integer tables of a 1-D plan (bit-exact with the reference):
+ * which = 0: Rader perm[k] = g^k mod p (rader.go:67-70), 1: Rader iperm,
+ * 2: Bluestein chirp index j*j mod 2n (bluestein.go:38), 3: Rader generator
+ * g and convolution length (2 values), 4: Bluestein convolution length m.
+ * Returns the table length (or -1 if the plan has no such table); copies at
+ * most cap entries. */
+GOFFT_API int64_t gofft_plan_table(const gofft_plan *p, int which, int64_t *out, int64_t cap);
+
+/* Spectrogram on device buffers in any precision (real type per precision):
+ * x has nx samples, window `segment` samples; out receives
+ * frames*(segment/2+1) densities; segment must be even. */
+GOFFT_API int gofft_spectrogram_device(int precision, const void *x, int64_t nx, int64_t segment,
+                             int64_t overlap, const void *window, double d, void *out,
+                             int64_t *nframes, gofft_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GOFFT_H */

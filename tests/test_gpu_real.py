@@ -1,0 +1,143 @@
+"""Real and multi-dimensional transforms on the B200 against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2, rng
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+F64_TOL = 1e-12
+F32_TOL = 1e-6
+
+REAL_N = [1, 2, 3, 4, 5, 6, 7, 8, 9, 12, 15, 16, 17, 31, 32, 100, 128, 1000, 1024, 2048, 2018, 4096, 1009,
+          131072, 20014]
+
+
+@pytest.mark.parametrize("n", REAL_N)
+def test_rfft_irfft_f64(n):
+    from fft_b200 import gofft as G
+    x = rng(n).standard_normal(n)
+    X = G.RFFT(x)
+    assert X.size == n // 2 + 1
+    assert rel_l2(X, O.rfft(x)) <= F64_TOL
+    back = G.IRFFT(X, n)
+    assert rel_l2(back, O.irfft(X, n)) <= F64_TOL
+    assert np.max(np.abs(back - x)) < 1e-9
+    p = G.NewRealPlan(n)
+    d = p.RFFT(np.zeros(n // 2 + 1, complex), x)
+    assert rel_l2(d, O.rfft(x)) <= F64_TOL
+
+
+def test_irfft_short_and_hermitian():
+    # rfft_test.go:105-124, 190-198
+    from fft_b200 import gofft as G
+    half = np.array([3, 1 - 2j, -0.5 + 0.4j, 2])
+    full = np.concatenate([half, np.conj(half[1:3][::-1])])
+    assert np.max(np.abs(G.IRFFT(half, 6) - np.real(O.ifft(full)))) < 1e-9
+    a = G.IRFFT(np.array([2 + 0j]), 4)
+    b = G.IRFFT(np.array([2 + 0j, 0, 0]), 4)
+    assert np.max(np.abs(a - b)) < 1e-12
+    for n in [8, 9, 1024]:
+        spec = rng(n).standard_normal(n // 2 + 1) + 1j * rng(n + 1).standard_normal(n // 2 + 1)
+        for k in [1, 2, n // 4 + 1, n // 2 + 1]:
+            assert rel_l2(G.IRFFT(spec[:k], n), O.irfft(spec[:k], n)) <= F64_TOL
+
+
+@pytest.mark.parametrize("shape", [(4, 6), (3, 5), (2, 8), (5, 4), (1, 1), (7, 3), (1, 6), (6, 1), (33, 17),
+                                   (1024, 1024), (512, 512), (9, 2018)])
+def test_rfft2_irfft2_f64(shape):
+    from fft_b200 import gofft as G
+    r, c = shape
+    x = rng(r * 1000 + c).standard_normal(r * c)
+    X = G.RFFT2(x, shape)
+    assert rel_l2(X, O.rfft2(x, r, c)) <= F64_TOL
+    back = G.IRFFT2(X, shape)
+    assert rel_l2(back, O.irfft2(X, r, c)) <= F64_TOL
+    assert np.max(np.abs(back - x)) < 1e-9
+    short = X[:-1]
+    assert rel_l2(G.IRFFT2(short, shape), O.irfft2(short, r, c)) <= F64_TOL
+
+
+@pytest.mark.parametrize("shape", [[2, 2], [3, 4], [4, 3], [1, 5], [5, 1], [2, 3, 4], [3, 1, 2], [2, 2, 2, 2],
+                                   [6, 5], [64, 64, 64], [17, 1009], [3, 65536]])
+def test_fftn_f64(shape):
+    from fft_b200 import gofft as G
+    n = int(np.prod(shape))
+    g = rng(n)
+    x = g.standard_normal(n) + 1j * g.standard_normal(n)
+    X = G.FFTN(x, shape)
+    assert rel_l2(X, O.fftn(x, shape)) <= F64_TOL
+    back = G.IFFTN(X, shape)
+    assert rel_l2(back, O.ifftn(X, shape)) <= F64_TOL
+    if len(shape) == 2:
+        assert rel_l2(G.FFT2(x, shape), X) <= F64_TOL
+        assert rel_l2(G.IFFT2(X, shape), back) <= F64_TOL
+
+
+def test_batched_rfft2_config2_shape():
+    # RFFT2 then IRFFT2 of 1024x1024 float64 images, batched on device
+    from fft_b200.device import DevicePlan
+    B = 3
+    x = rng(1).standard_normal((B, 1024, 1024))
+    p = DevicePlan("r2c", "f64", [1024, 1024], batch=B)
+    X = p.r2c(torch.from_numpy(x).cuda().reshape(B, -1))
+    got = X.cpu().numpy().reshape(B, 1024, 513)
+    for b in range(B):
+        assert rel_l2(got[b].ravel(), O.rfft2(x[b], 1024, 1024)) <= F64_TOL
+    back = p.c2r(X).cpu().numpy().reshape(B, 1024, 1024)
+    assert np.max(np.abs(back - x)) < 1e-12
+
+
+@pytest.mark.parametrize("prec", ["f32", "f32mixed"])
+def test_rfft2_fp32_forms(prec):
+    from fft_b200.device import DevicePlan
+    B, R, C = 4, 512, 512
+    x = rng(4).uniform(0, 1, (B, R, C)).astype(np.float32)
+    p = DevicePlan("r2c", prec, [R, C], batch=B)
+    X = p.r2c(torch.from_numpy(x).cuda().reshape(B, -1)).cpu().numpy().reshape(B, -1)
+    for b in range(B):
+        assert rel_l2(X[b], O.rfft2(x[b].astype(np.float64), R, C)) <= F32_TOL
+    back = p.c2r(torch.from_numpy(X).cuda()).cpu().numpy().reshape(B, R, C)
+    assert rel_l2(back, x) <= 2 * F32_TOL
+
+
+@pytest.mark.parametrize("prec", ["f32", "f32mixed"])
+def test_fftn_3d_fp32(prec):
+    from fft_b200.device import DevicePlan
+    s = [64, 64, 64]
+    g = rng(3)
+    x = ((g.standard_normal(s) + 1j * g.standard_normal(s)) / np.sqrt(2)).astype(np.complex64)
+    p = DevicePlan("c2c", prec, s)
+    X = p.c2c(torch.from_numpy(x).cuda()).cpu().numpy()
+    assert rel_l2(X.ravel(), O.fftn(x.astype(np.complex128), s)) <= F32_TOL
+    back = p.c2c(torch.from_numpy(X).cuda(), inverse=True).cpu().numpy()
+    assert rel_l2(back, x) <= 2 * F32_TOL
+
+
+def test_psd_and_spectrogram_f64(golden):
+    from fft_b200 import gofft as G
+    for n in [7, 8, 15, 32, 1024]:
+        x = rng(n).standard_normal(n)
+        assert rel_l2(G.PSD(x, 0.1), O.psd(x, 0.1)) <= F64_TOL
+    for seg, ov in [(8, 4), (32, 20), (2048, 1536), (15, 3)]:
+        x = rng(seg).standard_normal(20000)
+        w = O.hann(seg)
+        frames = G.Spectrogram(x, seg, ov, w, 0.5)
+        want = O.spectrogram(x, seg, ov, w, 0.5)
+        assert len(frames) == want.shape[0]
+        assert rel_l2(np.array(frames), want) <= F64_TOL
+    got = G.Spectrogram(golden["spec_in"], 32, 20, golden["spec_win"], 1.0)
+    np.testing.assert_allclose(np.array(got), golden["spec_out"], rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f32mixed"])
+def test_device_spectrogram_fp32(prec):
+    from fft_b200.device import spectrogram
+    x = rng(3).standard_normal(1 << 16).astype(np.float32)
+    w = O.hann(2048).astype(np.float32)
+    got = spectrogram(torch.from_numpy(x).cuda(), 2048, 1536, torch.from_numpy(w).cuda(), 1.0, prec)
+    want = O.spectrogram(x.astype(np.float64), 2048, 1536, w.astype(np.float64), 1.0)
+    assert got.shape == want.shape
+    assert rel_l2(got.cpu().numpy(), want) <= F32_TOL

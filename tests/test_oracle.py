@@ -1,0 +1,143 @@
+"""The oracle (C restatement of go-fft/fft) pinned against the golden
+vectors (numpy.fft under the reference's own gate, rtol 1e-9 / atol 1e-7,
+benchmarks/verify_correctness.py:16-17) and the reference's known answers."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from oracle import oracle as O
+
+RTOL, ATOL = 1e-9, 1e-7
+
+
+def close(got, want):
+    np.testing.assert_allclose(got, want, rtol=RTOL, atol=ATOL)
+
+
+def test_c2c_golden(golden):
+    for k in golden:
+        if k.startswith("c2c_in_"):
+            n = int(k.split("_")[-1])
+            x = golden[k]
+            close(O.fft(x), golden["c2c_fft_%d" % n])
+            close(O.ifft(x), golden["c2c_ifft_%d" % n])
+
+
+def test_real_golden(golden):
+    for k in golden:
+        if k.startswith("r_in_"):
+            n = int(k.split("_")[-1])
+            close(O.rfft(golden[k]), golden["r_rfft_%d" % n])
+            close(O.irfft(golden["r_spec_%d" % n], n), golden["r_irfft_%d" % n])
+            close(O.psd(golden[k], 0.25), golden["r_psd_%d" % n])
+
+
+def test_2d_nd_golden(golden):
+    for k in golden:
+        if k.startswith("r2_in_"):
+            key = k[len("r2_in_"):]
+            r, c = map(int, key.split("x"))
+            close(O.rfft2(golden[k], r, c).reshape(r, c // 2 + 1), golden["r2_rfft2_" + key])
+            back = O.irfft2(O.rfft2(golden[k], r, c), r, c).reshape(r, c)
+            close(back, golden["r2_irfft2_" + key])
+        if k.startswith("nd_in_"):
+            key = k[len("nd_in_"):]
+            shape = list(map(int, key.split("x")))
+            close(O.fftn(golden[k], shape).reshape(shape), golden["nd_fftn_" + key])
+            close(O.ifftn(golden[k], shape).reshape(shape), golden["nd_ifftn_" + key])
+
+
+def test_spectrogram_golden(golden):
+    got = O.spectrogram(golden["spec_in"], 32, 20, golden["spec_win"], 1.0)
+    close(got, golden["spec_out"])
+
+
+def test_known_answers(kat):
+    assert list(O.bit_reverse_perm(8)) == kat["bit_reverse_8"]["value"]
+    for p, g in kat["primitive_root"]["value"].items():
+        assert O.primitive_root(int(p)) == g
+    for n, f in kat["factorize"]["value"].items():
+        assert O.factorize(int(n)) == f
+    for n, v in kat["factors_small"]["value"].items():
+        assert O.factors_small(int(n)) == v
+    for n, v in kat["is_prime"]["value"].items():
+        assert O.is_prime(int(n)) == v
+    assert O.ENGINE_NAMES[O.engine(641)] == "bluestein"
+    assert O.ENGINE_NAMES[O.engine(769)] == "rader"
+    for n in kat["rader_cyclic"]["value"]:
+        info = O.rader_info(n)
+        assert info["cyclic"] and info["cl"] == n - 1
+    for n in kat["rader_linear"]["value"]:
+        info = O.rader_info(n)
+        assert not info["cyclic"] and info["cl"] >= 2 * (n - 1) and O.conv_cost(info["cl"])[1]
+    for m in kat["conv_cost_not_ok"]["value"]:
+        assert not O.conv_cost(m)[1]
+    for m in kat["conv_cost_ok"]["value"]:
+        assert O.conv_cost(m)[1]
+    assert O.rader_info(10007)["cl"] == kat["rader_10007_cl"]["value"]
+    np.testing.assert_allclose(O.hann(5), kat["hann_5"]["value"], atol=1e-15)
+    assert O.spectrogram(np.sin(np.arange(20.0)), 8, 4, O.hann(8), 1.0).shape[0] == 4
+
+
+def test_best_conv_len_is_argmin():
+    # radix7_test.go:153-184: bestConvLen is the argmin of convCost over its window
+    for lo in [1, 2, 16, 10004, 19944, 20012, 100000]:
+        g = O.best_conv_len(lo)
+        gc, ok = O.conv_cost(g)
+        assert ok and g >= lo
+        hi = lo + (lo * 4 + 9) // 10
+        for m in range(lo, hi + 1):
+            c, ok2 = O.conv_cost(m)
+            assert not (ok2 and c < gc)
+
+
+def test_rader_tables_are_permutations():
+    for p in [769, 1009, 2017, 10007]:
+        info = O.rader_info(p)
+        q = p - 1
+        assert sorted(info["perm"]) == list(range(1, p))
+        assert sorted(info["iperm"]) == list(range(1, p))
+        # iperm[q] = perm[(q - qi) mod q] (rader.go:72-74)
+        for qi in range(0, q, 97):
+            assert info["iperm"][qi] == info["perm"][(q - qi) % q]
+
+
+def test_chirp_index():
+    for n in [17, 641, 1000, 10007]:
+        jj = O.chirp_index(n)
+        j = np.arange(n, dtype=np.int64)
+        assert np.array_equal(jj, (j * j) % (2 * n))
+
+
+def test_engines_cross_check():
+    # rader_test.go:80-96: Rader and Bluestein agree on the large primes
+    g = np.random.default_rng(7)
+    for n in [769, 1009, 2017, 10007]:
+        x = g.uniform(-1, 1, n) + 1j * g.uniform(-1, 1, n)
+        a = O.rader(x)
+        b = O.bluestein(x)
+        # the reference's tolerance: max |diff| <= 1e-13 n^2 (rader_test.go:22)
+        assert np.max(np.abs(a - b)) <= 1e-13 * n * n
+        assert rel_l2(a, np.fft.fft(x)) < 1e-13
+
+
+def test_naive_dft_small():
+    # fft_test.go:12-24: O(N^2) DFT oracle for small n
+    for n in range(1, 40):
+        x = np.sin(np.arange(n) * 0.7) + (np.arange(n) % 3) + 1j * np.cos(np.arange(n) * 0.3)
+        k = np.arange(n)
+        naive = (x[None, :] * np.exp(-2j * np.pi * np.outer(k, k) / n)).sum(axis=1)
+        assert np.max(np.abs(O.fft(x) - naive)) < 1e-9
+
+
+@pytest.mark.parametrize("workers", [1, 3, 8])
+def test_parallel_matches_serial(workers):
+    # parallel_test.go:64-106: worker count never changes results
+    g = np.random.default_rng(3)
+    x = g.standard_normal((64, 300))
+    O.set_workers(1)
+    a = O.rfft2(x, 64, 300)
+    O.set_workers(workers)
+    b = O.rfft2(x, 64, 300)
+    O.set_workers(0)
+    assert np.array_equal(a, b)
