@@ -1,0 +1,374 @@
+"""Benchmark: batched RFFT2 -> IRFFT2 of 1024x1024 float64 images on B200.
+
+One step is RFFT2 followed by IRFFT2 over a batch of images (the 2-D real
+round trip of go-fft's rfft2.go:22-138), inputs resident in HBM and larger
+than L2, so every step streams from HBM.  The headline is GB/s of compulsory
+bytes (input + output of each transform: 33,587,200 B per image round trip).
+The same step is then timed in the FP32-mixed form (complex64, hi+lo
+twiddles), whose ratio to the FP64 form and relative L2 error against the
+FP64 oracle are reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --impl reference the C restatement of go-fft (the oracle; Go is absent
+on this machine) is timed on the host cores on the same workload.  Under
+torchrun each rank processes its own batch (weak scaling, no collective on
+the data path); rank 0 prints one JSON line.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ROWS, COLS = 1024, 1024
+RC = COLS // 2 + 1
+METRIC = "batched FFT GB/s vs HBM peak; FP32-mixed vs plain FP64 at stated rel-L2 error"
+WORKLOAD = "RFFT2+IRFFT2 round trip, 1024x1024 float64 images (rfft2.go:22-138)"
+
+
+def algo_bytes(prec_bytes):
+    """Compulsory bytes of one image round trip: RFFT2 reads R*C reals and
+    writes R*(C/2+1) complex; IRFFT2 the reverse."""
+    real = ROWS * COLS * prec_bytes
+    cplx = ROWS * RC * 2 * prec_bytes
+    return 2 * (real + cplx)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def gen_images(b, seed=1):
+    """float64 images: i.i.d. N(0,1) from `seed` plus a sum of 8 sinusoids
+    with integer frequencies in [1,200] and amplitudes in [0.5,2] drawn from
+    the same stream after the noise."""
+    g = np.random.default_rng(seed)
+    x = g.standard_normal((b, ROWS, COLS))
+    f = g.integers(1, 201, size=8)
+    h = g.integers(1, 201, size=8)
+    a = g.uniform(0.5, 2.0, size=8)
+    r = np.arange(ROWS)[:, None] / ROWS
+    c = np.arange(COLS)[None, :] / COLS
+    s = np.zeros((ROWS, COLS))
+    for i in range(8):
+        s += a[i] * np.sin(2 * np.pi * (f[i] * r + h[i] * c))
+    return x + s[None]
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during a timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        try:
+            rows = [l.strip().split(",") for l in open(self.path) if l.strip()]
+        except Exception:
+            return out
+        sm, reasons = [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                out["sm_max_mhz"] = float(r[2])
+                for i, nm in enumerate(names):
+                    if r[5 + i].strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                pass
+        if sm:
+            out["sm_mhz"] = statistics.median(sm)
+            out["samples"] = len(sm)
+        out["reasons"] = sorted(reasons)
+        return out
+
+
+def dist_setup(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and not dist.is_initialized():
+        import datetime
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU arms (the oracle: C restatement of go-fft, all host threads)
+# ---------------------------------------------------------------------------
+def cpu_time_images(n_images, seed=1):
+    from oracle import oracle as O
+    x = gen_images(n_images, seed)
+    t0 = time.perf_counter()
+    O.batch_rfft2_roundtrip(x)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(budget_s=10.0):
+    """The oracle on all host cores over repeated passes of an 8-image batch
+    until about budget_s of CPU work."""
+    from oracle import oracle as O
+    O.set_workers(0)
+    cores = O.get_workers()
+    x = gen_images(8, 1)
+    O.batch_rfft2_roundtrip(x[:1])
+    passes, t = 0, 0.0
+    while t < budget_s and passes < 1000:
+        t0 = time.perf_counter()
+        O.batch_rfft2_roundtrip(x)
+        t += time.perf_counter() - t0
+        passes += 1
+    n = passes * x.shape[0]
+    gbs = n * algo_bytes(8) / t / 1e9
+    return {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+            "sample": "%d passes over 8 images of the 1024x1024 float64 RFFT2+IRFFT2 round trip (%.1f s)"
+                      % (passes, t),
+            "transforms_per_s": round(2 * n / t, 2)}
+
+
+def run_reference(args):
+    world, rank, _ = (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    O.set_workers(0)
+    cores = O.get_workers()
+    per_step = 2
+    x = gen_images(per_step, 1)
+    for _ in range(args.warmup):
+        O.batch_rfft2_roundtrip(x)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.batch_rfft2_roundtrip(x)
+    t = time.perf_counter() - t0
+    gbs = args.steps * per_step * algo_bytes(8) / t / 1e9
+    line = {"metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * t / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "images_per_step": per_step, "rows": ROWS, "cols": COLS},
+            "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+                             "sample": "%d images per step x %d steps (C restatement of go-fft; no Go "
+                                       "toolchain on this machine)" % (per_step, args.steps)},
+            "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def time_pipeline(plan, x, spec, back, steps, warmup, world, flush=None):
+    import torch
+    for _ in range(warmup):
+        plan.r2c(x, out=spec)
+        plan.c2r(spec, out=back)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        plan.r2c(x, out=spec)
+        plan.c2r(spec, out=back)
+    e1.record(s)
+    torch.cuda.synchronize()
+    barrier(world)
+    return e0.elapsed_time(e1) / 1e3
+
+
+def run_ours(args):
+    import torch
+    from fft_b200 import _lib
+    from fft_b200.device import DevicePlan
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    B = args.batch
+    peak, peak_kind = peaks()
+
+    # FP64 form: inputs in HBM, 2 x 268 MB per direction > L2
+    x64 = torch.from_numpy(gen_images(B, 1 + rank)).cuda().reshape(B, -1)
+    p64 = DevicePlan("r2c", "f64", [ROWS, COLS], batch=B)
+    s64 = torch.empty((B, ROWS * RC), dtype=torch.complex128, device="cuda")
+    b64 = torch.empty_like(x64)
+
+    n0 = _lib.launch_count()
+    with Clocks(local) as clk:
+        t64 = time_pipeline(p64, x64, s64, b64, args.steps, args.warmup, world)
+    launches = (_lib.launch_count() - n0) * args.steps // (args.steps + args.warmup)
+    t64 = max_over_ranks(t64, world)
+    gbs64 = world * args.steps * B * algo_bytes(8) / t64 / 1e9
+
+    # FP32-mixed form on the same images (rounded to float32)
+    x32 = x64.to(torch.float32)
+    p32 = DevicePlan("r2c", "f32mixed", [ROWS, COLS], batch=B)
+    s32 = torch.empty((B, ROWS * RC), dtype=torch.complex64, device="cuda")
+    b32 = torch.empty_like(x32)
+    t32 = time_pipeline(p32, x32, s32, b32, args.steps, args.warmup, world)
+    t32 = max_over_ranks(t32, world)
+    gbs32 = world * args.steps * B * algo_bytes(4) / t32 / 1e9
+
+    # per-kernel timing of the FP64 step with CUDA events (separate pass)
+    _lib.timing_enable(True)
+    _lib.timing_report()
+    for _ in range(max(3, min(args.steps, 20))):
+        p64.r2c(x64, out=s64)
+        p64.c2r(s64, out=b64)
+    torch.cuda.synchronize()
+    rep = _lib.timing_report()
+    _lib.timing_enable(False)
+    dom = max(rep, key=lambda r: r["ms"])
+    total_ms = sum(r["ms"] for r in rep)
+    achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9
+
+    # accuracy on image 0: FP64 GPU vs oracle, FP32-mixed vs the FP64 oracle
+    from oracle import oracle as O
+    img0 = x64[0].cpu().numpy()
+    want = O.rfft2(img0, ROWS, COLS)
+    got64 = s64[0].cpu().numpy()
+    rel64 = float(np.linalg.norm(got64 - want) / np.linalg.norm(want))
+    got32 = s32[0].cpu().numpy().astype(np.complex128)
+    want32 = O.rfft2(x32[0].cpu().numpy().astype(np.float64), ROWS, COLS)
+    rel32 = float(np.linalg.norm(got32 - want32) / np.linalg.norm(want32))
+    maxabs32 = float(np.max(np.abs(got32 - want32)))
+    rt64 = float(torch.max(torch.abs(b64[0] - x64[0])).item())
+
+    # end to end through the C-ABI with pinned host buffers (copies timed)
+    e2e = None
+    if rank == 0 or world > 1:
+        hx = x64.cpu().pin_memory()
+        hs = torch.empty((B, ROWS * RC), dtype=torch.complex128).pin_memory()
+        hb = torch.empty_like(hx).pin_memory()
+        pe = DevicePlan("r2c", "f64", [ROWS, COLS], batch=B)
+        for _ in range(2):
+            pe.r2c_host(hx.data_ptr(), hs.data_ptr())
+            pe.c2r_host(hs.data_ptr(), hb.data_ptr())
+        ke = max(2, args.steps // 4)
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            pe.r2c_host(hx.data_ptr(), hs.data_ptr())
+            pe.c2r_host(hs.data_ptr(), hb.data_ptr())
+        te = max_over_ranks(time.perf_counter() - t0, world)
+        e2e = {"value": round(world * ke * B * algo_bytes(8) / te / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": B * (ROWS * COLS * 8 + ROWS * RC * 16),
+               "d2h_bytes_per_step": B * (ROWS * RC * 16 + ROWS * COLS * 8),
+               "ms_per_step": round(1e3 * te / ke, 3), "timer": "host wall clock (pinned buffers)"}
+        pe.close()
+
+    if rank != 0:
+        return 0
+    cpu = cpu_baseline() if world == 1 else None
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": round(gbs64, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * t64 / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "images_per_step_per_gpu": B, "rows": ROWS, "cols": COLS,
+                   "l2": "inputs larger than L2 (%.0f MB per direction per GPU)" % (B * ROWS * COLS * 8 / 1e6),
+                   "parallelism": "replicas" if world == 1 else "batch-sharded x%d" % world},
+        "transforms_per_s": round(world * args.steps * B * 2 / t64, 1),
+        "hbm_frac": round(gbs64 / world / peak, 4),
+        "rel_l2_f64_vs_oracle": rel64, "roundtrip_max_abs_f64": rt64,
+        "mixed": {"value": round(gbs32, 2), "unit": "GB/s", "dtype": "f32 (hi+lo twiddles)",
+                  "transforms_per_s": round(world * args.steps * B * 2 / t32, 1),
+                  "speedup_vs_f64": round(t64 / t32, 3), "rel_l2_vs_f64_oracle": rel32,
+                  "max_abs_vs_f64_oracle": maxabs32, "ms_per_step": round(1e3 * t32 / args.steps, 4)},
+        "roofline": {"bound": "hbm", "kernel": dom["kernel"], "achieved": round(achieved, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "peak_source": peak_kind, "traffic": None,
+                     "share": round(dom["ms"] / total_ms, 3),
+                     "kernels": [{"kernel": r["kernel"], "launches": r["launches"],
+                                  "avg_us": round(1e3 * r["ms"] / r["launches"], 2),
+                                  "gbs": round(r["bytes"] / (r["ms"] / 1e3) / 1e9, 1),
+                                  "share": round(r["ms"] / total_ms, 3)} for r in rep]},
+        "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu,
+    }
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=32, help="images per step per GPU")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

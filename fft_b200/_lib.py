@@ -61,6 +61,10 @@ SIGNATURES = {
     "gofft_plan_table": (_i64, [_vp, ctypes.c_int, _i64p, _i64]),
     "gofft_spectrogram_device": (ctypes.c_int, [ctypes.c_int, _vp, _i64, _i64, _i64, _vp, ctypes.c_double, _vp,
                                                 _i64p, _vp]),
+    "gofft_launch_count": (_i64, []),
+    "gofft_timing_enable": (ctypes.c_int, [ctypes.c_int]),
+    "gofft_timing_report": (_i64, [ctypes.c_char_p, _i64]),
+    "gofft_set_lines_per_cta": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
 }
 
 _lib = None
@@ -99,3 +103,21 @@ def check(status):
     if status != GOFFT_OK:
         raise GoFFTError(status, last_error())
     return status
+
+
+def launch_count():
+    """Engine kernels launched by this process so far."""
+    return int(lib().gofft_launch_count())
+
+
+def timing_enable(on=True):
+    lib().gofft_timing_enable(1 if on else 0)
+
+
+def timing_report():
+    """Per-kernel CUDA-event timings since the last call (list of dicts)."""
+    import json
+    n = lib().gofft_timing_report(None, 0)
+    buf = ctypes.create_string_buffer(int(n) + 1)
+    lib().gofft_timing_report(buf, n + 1)
+    return json.loads(buf.value.decode() or "[]")

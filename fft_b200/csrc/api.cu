@@ -713,3 +713,27 @@ extern "C" int gofft_spectrogram(const double *x, int64_t nx, int64_t segment, i
   }
   return GOFFT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Instrumentation
+// ---------------------------------------------------------------------------
+extern "C" int64_t gofft_launch_count(void) { return launch_count(); }
+extern "C" int gofft_timing_enable(int on) {
+  timing_enable(on);
+  return GOFFT_OK;
+}
+extern "C" int64_t gofft_timing_report(char *buf, int64_t cap) {
+  static thread_local std::string last;
+  if (!buf || cap <= 0) {
+    last = timing_report();
+    return (int64_t)last.size();
+  }
+  const size_t k = std::min<size_t>(last.size(), (size_t)cap - 1);
+  memcpy(buf, last.data(), k);
+  buf[k] = 0;
+  return (int64_t)last.size();
+}
+extern "C" int gofft_set_lines_per_cta(int precision, int64_t n, int op, int colmode, int lpc) {
+  set_lpc_override(precision, n, op, colmode, lpc);
+  return GOFFT_OK;
+}

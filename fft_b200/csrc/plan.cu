@@ -1,5 +1,6 @@
 // plan.cu -- line programs, 1-D executors and real executors.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <sstream>
@@ -284,6 +285,76 @@ std::shared_ptr<DevProg> get_prog(long long n, int prec) {
 }
 
 // ---------------------------------------------------------------------------
+// Instrumentation: a launch counter and optional CUDA-event timing of every
+// line-kernel launch (events recorded on the launch stream around it).
+// ---------------------------------------------------------------------------
+static std::atomic<long long> g_launches{0};
+static std::atomic<int> g_timing{0};
+struct TimingRec {
+  std::string key;
+  cudaEvent_t a, b;
+  double bytes;
+};
+static std::mutex g_tmu;
+static std::vector<TimingRec> g_trecs;
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(); }
+void timing_enable(int on) { g_timing.store(on ? 1 : 0); }
+
+std::string timing_report() {
+  std::vector<TimingRec> recs;
+  {
+    std::lock_guard<std::mutex> lk(g_tmu);
+    recs.swap(g_trecs);
+  }
+  struct Agg { long long launches = 0; double ms = 0, bytes = 0; };
+  std::map<std::string, Agg> agg;
+  for (auto &r : recs) {
+    float ms = 0;
+    cudaEventSynchronize(r.b);
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    Agg &g = agg[r.key];
+    g.launches++;
+    g.ms += ms;
+    g.bytes += r.bytes;
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  std::ostringstream o;
+  o << "[";
+  bool first = true;
+  for (auto &kv : agg) {
+    o << (first ? "" : ",") << "{\"kernel\":\"" << kv.first << "\",\"launches\":" << kv.second.launches
+      << ",\"ms\":" << kv.second.ms << ",\"bytes\":" << kv.second.bytes << "}";
+    first = false;
+  }
+  o << "]";
+  return o.str();
+}
+
+static const char *op_name(int op) {
+  static const char *n[] = {"c2c", "c2c_twiddle", "r2c_packed", "c2r_packed", "r2c_full",
+                            "c2r_full", "rader_fused", "bluestein_fused", "spectrogram"};
+  return (op >= 0 && op < OP_COUNT) ? n[op] : "?";
+}
+
+// Compulsory bytes (input + output) of one launch.
+static double algo_bytes(int op, const DevProg &dp, const KArgs &a, long long nl) {
+  const double c = (double)csize(dp.prec), r = (double)rsize(dp.prec), n = dp.n;
+  switch (op) {
+    case OP_R2C:
+    case OP_C2R: return nl * (2 * n * r + (n + 1) * c);
+    case OP_R2C_FULL:
+    case OP_C2R_FULL: return nl * (n * r + (double)(dp.n / 2 + 1) * c);
+    case OP_RADER:
+    case OP_BLUE: return 2.0 * nl * (double)a.ia * c;
+    case OP_SPECTRO: return nl * (2 * n * r + (n + 1) * r);
+    default: return 2.0 * nl * n * c;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Launch
 // ---------------------------------------------------------------------------
 static std::mutex g_lpc_mu;
@@ -337,8 +408,25 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   if (!f) return set_err(5, "no kernel instance for this precision/op");
   if (int rc = ensure_smem(f, smem)) return rc;
   const long long grid = (nlines + lpc - 1) / lpc;
+  count_launch();
+  TimingRec rec;
+  const bool timed = g_timing.load() != 0;
+  if (timed) {
+    cudaEventCreate(&rec.a);
+    cudaEventCreate(&rec.b);
+    cudaEventRecord(rec.a, st);
+  }
   f<<<(unsigned)grid, lpc * dp.lp.T, smem, st>>>(a);
   GF_CK(cudaGetLastError());
+  if (timed) {
+    cudaEventRecord(rec.b, st);
+    std::ostringstream k;
+    k << op_name(op) << "/n=" << dp.n << "/prec=" << dp.prec << "/lpc=" << lpc << "/T=" << dp.lp.T;
+    rec.key = k.str();
+    rec.bytes = algo_bytes(op, dp, a, nlines);
+    std::lock_guard<std::mutex> lk(g_tmu);
+    g_trecs.push_back(rec);
+  }
   return 0;
 }
 
@@ -372,9 +460,10 @@ static bool side_simple(const Side &s, long long &D) {
 
 static char *align256(char *p) { return (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255); }
 
-#define GF_PREC_CALL(prec, fn, ...)                                        \
-  ((prec) == F64 ? prec_f64::fn(__VA_ARGS__)                               \
-                 : ((prec) == F32 ? prec_f32::fn(__VA_ARGS__) : prec_f32c::fn(__VA_ARGS__)))
+#define GF_PREC_CALL(prec, fn, ...)                                                \
+  (count_launch(), (prec) == F64 ? prec_f64::fn(__VA_ARGS__)                       \
+                                 : ((prec) == F32 ? prec_f32::fn(__VA_ARGS__)      \
+                                                  : prec_f32c::fn(__VA_ARGS__)))
 
 int Exec1D::exec(const Side &in, const Side &out, long long nl, int cji, int cjo, double scale,
                  void *ws, cudaStream_t st) const {

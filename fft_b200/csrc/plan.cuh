@@ -114,6 +114,12 @@ inline Side mk_side(void *p, long long dist_b, long long dist_l, long long strid
 // Contiguous lines of length len.
 inline Side contig(void *p, long long len) { return mk_side(p, len, 0, 1, 1); }
 
+// Instrumentation (launch counter, CUDA-event timing per line kernel).
+void count_launch();
+long long launch_count();
+void timing_enable(int on);
+std::string timing_report();
+
 // Autotuned lines-per-CTA overrides (key: prec, n, op, column-mode).
 void set_lpc_override(int prec, long long n, int op, int colmode, int lpc);
 int get_lpc_override(int prec, long long n, int op, int colmode);

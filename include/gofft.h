@@ -176,6 +176,24 @@ GOFFT_API int gofft_spectrogram_device(int precision, const void *x, int64_t nx,
                              int64_t overlap, const void *window, double d, void *out,
                              int64_t *nframes, gofft_stream stream);
 
+/* ------------------------------------------------------------------------ */
+/* 3. Instrumentation and tuning (no counterpart in the reference).          */
+/* ------------------------------------------------------------------------ */
+
+/* Number of engine kernels launched by this process so far. */
+GOFFT_API int64_t gofft_launch_count(void);
+/* Turn CUDA-event timing of every line-kernel launch on (1) or off (0): an
+ * event pair is recorded on the launch stream around each launch. */
+GOFFT_API int gofft_timing_enable(int on);
+/* Collects the timed launches since the last report (synchronising on their
+ * events) as JSON [{kernel, launches, ms, bytes}], bytes being the
+ * compulsory input+output bytes.  Call once with buf == NULL to aggregate and
+ * get the length, then again with a buffer to copy it. */
+GOFFT_API int64_t gofft_timing_report(char *buf, int64_t cap);
+/* Overrides the lines-per-CTA of the line kernel for (precision, length n,
+ * op, column mode); lpc <= 0 restores the heuristic.  Used by the autotuner. */
+GOFFT_API int gofft_set_lines_per_cta(int precision, int64_t n, int op, int colmode, int lpc);
+
 #ifdef __cplusplus
 }
 #endif
