@@ -634,6 +634,7 @@ static int spectro_dev(int prec, const void *x, int64_t nx, int64_t seg, int64_t
   a.aux0 = rx->tw2;
   a.aux1 = win;
   a.scale = d / (double)seg;
+  a.ic = pairs_aligned(a.in, prec) ? GF_PAIR_ALIGNED : 0;
   (void)nx;
   return launch_line(OP_SPECTRO, *rx->cx->prog, a, frames, st);
 }

@@ -81,7 +81,7 @@ struct KArgs {
 // ---------------------------------------------------------------------------
 template <class P, int R, int MAXE>
 GF_DEV void stage(typename P::cpx (&v)[MAXE], typename P::cpx *s, int n, int T, int ns,
-                  FastDiv nsd, const typename P::tw_t *tw, int t) {
+                  FastDiv nsd, const typename P::tw_t *tw, int t, bool cj) {
   using C = typename P::cpx;
   constexpr int NB = MAXE / R;
   const int nb = n / R;
@@ -90,7 +90,11 @@ GF_DEV void stage(typename P::cpx (&v)[MAXE], typename P::cpx *s, int n, int T, 
     const int j = t + b * T;
     if (j < nb) {
 #pragma unroll
-      for (int r = 0; r < R; r++) v[b * R + r] = s[spad(j + r * nb)];
+      for (int r = 0; r < R; r++) {
+        C x = s[spad(j + r * nb)];
+        if (cj) x.y = -x.y;
+        v[b * R + r] = x;
+      }
     }
   }
   __syncthreads();
@@ -117,26 +121,33 @@ GF_DEV void stage(typename P::cpx (&v)[MAXE], typename P::cpx *s, int n, int T, 
 // Runs every stage of lp on the line buffer s.  All threads of the CTA call
 // this (stages contain CTA barriers).  One register array serves every radix:
 // giving each radix case its own array makes ptxas allocate the switch
-// alternatives jointly and spill.
+// alternatives jointly and spill.  cj_first conjugates the inputs of the
+// first stage (or, for a stage-less line of length 1, the element itself).
 template <class P, int MAXE>
-GF_DEV void run_stages(typename P::cpx *s, const LineProg &lp, int t) {
+GF_DEV void run_stages(typename P::cpx *s, const LineProg &lp, int t, bool cj_first) {
   using TW = typename P::tw_t;
   typename P::cpx v[MAXE];
   const int n = lp.n, T = lp.T;
+  if (lp.nst == 0) {
+    if (cj_first && t == 0) s[0].y = -s[0].y;
+    __syncthreads();
+    return;
+  }
   for (int si = 0; si < lp.nst; si++) {
     const int ns = lp.ns[si];
     const FastDiv nsd = lp.nsdiv[si];
     const TW *tw = (const TW *)lp.tw + lp.twoff[si];
+    const bool cj = cj_first && si == 0;
     switch (lp.radix[si]) {
-      case 2: stage<P, 2, MAXE>(v, s, n, T, ns, nsd, tw, t); break;
-      case 3: stage<P, 3, MAXE>(v, s, n, T, ns, nsd, tw, t); break;
-      case 4: stage<P, 4, MAXE>(v, s, n, T, ns, nsd, tw, t); break;
-      case 5: stage<P, 5, MAXE>(v, s, n, T, ns, nsd, tw, t); break;
-      case 7: stage<P, 7, MAXE>(v, s, n, T, ns, nsd, tw, t); break;
-      case 8: stage<P, 8, MAXE>(v, s, n, T, ns, nsd, tw, t); break;
-      case 11: stage<P, 11, MAXE>(v, s, n, T, ns, nsd, tw, t); break;
-      case 13: stage<P, 13, MAXE>(v, s, n, T, ns, nsd, tw, t); break;
-      case 16: stage<P, 16, MAXE>(v, s, n, T, ns, nsd, tw, t); break;
+      case 2: stage<P, 2, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
+      case 3: stage<P, 3, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
+      case 4: stage<P, 4, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
+      case 5: stage<P, 5, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
+      case 7: stage<P, 7, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
+      case 8: stage<P, 8, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
+      case 11: stage<P, 11, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
+      case 13: stage<P, 13, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
+      case 16: stage<P, 16, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
       default: break;
     }
   }
@@ -179,22 +190,57 @@ template <class P> GF_DEV typename P::cpx *line_extra(int l, int n, int lpc) {
 }
 
 // ---------------------------------------------------------------------------
-// Ops: prologue (global -> smem) and epilogue (smem -> global).
+// Asynchronous global -> shared copies (cp.async): a tile's loads are all in
+// flight before any thread waits, so the prologue is bandwidth- rather than
+// latency-bound.  Data that needs arithmetic on arrival (conjugation, chirp,
+// window, real-spectrum folding) is copied raw and fixed up in shared memory.
+// ---------------------------------------------------------------------------
+GF_DEV void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+GF_DEV void cp_async8(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+GF_DEV void cp_async4(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+GF_DEV void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+// One element of `bytes` (4, 8 or 16).
+template <int BYTES> GF_DEV void cp_async_n(void *s, const void *g) {
+  if constexpr (BYTES == 16) cp_async16(s, g);
+  else if constexpr (BYTES == 8) cp_async8(s, g);
+  else cp_async4(s, g);
+}
+
+// KArgs::ic bit used by the real-input ops: real pairs are aligned to the
+// pair size, so a pair moves as one vector copy.
+#define GF_PAIR_ALIGNED 0x40000000
+
+// ---------------------------------------------------------------------------
+// Ops.  load() issues the prologue copies (completed by the kernel before
+// prep()); prep() runs in-shared-memory fix-ups and ends with a barrier when it
+// does anything; store() is the epilogue.  first_conj() asks the first Stockham
+// stage to conjugate what it reads (the inverse via conj(DFT(conj x))).
 // ---------------------------------------------------------------------------
 
 // Plain complex line: optional conjugation (inverse) and scale.
 struct OpC2C {
+  static constexpr bool kConv = false;
+  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
     using C = typename P::cpx;
     const C *in = (const C *)a.in.ptr;
     const int n = a.lp.n;
-    const bool cj = a.cj_in;
     tile_loop(a.in, a.lpc, n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      C x = in[off];
-      if (cj) x.y = -x.y;
-      line_buf<P>(l, n)[spad(i)] = x;
+      cp_async_n<sizeof(C)>(&line_buf<P>(l, n)[spad(i)], &in[off]);
     });
   }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
   template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
     using C = typename P::cpx;
     using Rl = typename P::real;
@@ -212,9 +258,12 @@ struct OpC2C {
 // Four-step pass 1 epilogue: element k1 of line n2 (line index within its
 // batch) is multiplied by W_N^{n2*k1} from the table aux0 (N entries).
 struct OpC2CTwiddle {
+  static constexpr bool kConv = false;
+  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
     OpC2C::load<P>(a, line0);
   }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
   template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
     using C = typename P::cpx;
     using TW = typename P::tw_t;
@@ -233,24 +282,37 @@ struct OpC2CTwiddle {
   }
 };
 
+// Copies the real pair (x[2j], x[2j+1]) of a line into complex slot j.
+template <class P>
+GF_DEV void load_real_pair(const KArgs &a, typename P::cpx *dst, long long base, long long st) {
+  using Rl = typename P::real;
+  const Rl *in = (const Rl *)a.in.ptr;
+  if (a.ic & GF_PAIR_ALIGNED) {
+    cp_async_n<2 * sizeof(Rl)>(dst, &in[base]);
+  } else {
+    cp_async_n<sizeof(Rl)>(&dst->x, &in[base]);
+    cp_async_n<sizeof(Rl)>(&dst->y, &in[base + st]);
+  }
+}
+
 // Even-length real forward: the 2m reals of a line are read as m complex
 // values z[j] = x[2j] + i x[2j+1]; after the m-point FFT the untangle
 //   X[k] = (Z[k] + conj Z[m-k])/2 + W_2m^k (Z[k] - conj Z[m-k])/(2i)
 // writes bins 0..m (aux0 = W_2m^k table, k = 0..m).  Sides count reals on
 // input and complex bins on output.
 struct OpR2CPacked {
+  static constexpr bool kConv = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    const Rl *in = (const Rl *)a.in.ptr;
     const int m = a.lp.n;
     const long long st = a.in.stride;
     tile_loop(a.in, a.lpc, m, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
       // off addresses element j with stride st; the real pair is at 2j, 2j+1
       const long long base = off - (long long)j * st + 2LL * j * st;
-      line_buf<P>(l, m)[spad(j)] = mkc(in[base], in[base + st]);
+      load_real_pair<P>(a, &line_buf<P>(l, m)[spad(j)], base, st);
     });
   }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
   template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
     using C = typename P::cpx;
     using Rl = typename P::real;
@@ -281,48 +343,65 @@ struct OpR2CPacked {
   }
 };
 
+GF_DEV double2 cconj_tw(double2 w) { return make_double2(w.x, -w.y); }
+GF_DEV float2 cconj_tw(float2 w) { return make_float2(w.x, -w.y); }
+GF_DEV float4 cconj_tw(float4 w) { return make_float4(w.x, -w.y, w.z, -w.w); }
+
+// Copies bins 0..min(nb, cnt)-1 of each line raw into slots 0.., zeroing the
+// slots of missing bins up to cnt.
+template <class P>
+GF_DEV void load_bins(const KArgs &a, long long line0, int slots, int cnt, int nb) {
+  using C = typename P::cpx;
+  using Rl = typename P::real;
+  const C *in = (const C *)a.in.ptr;
+  tile_loop(a.in, a.lpc, cnt, FastDiv((uint32_t)cnt), a.lpcdiv, line0, a.nlines,
+            [&](int l, int k, long long off) {
+              C *d = &line_buf<P>(l, slots)[spad(k)];
+              if (k < nb) cp_async_n<sizeof(C)>(d, &in[off]);
+              else *d = mkc((Rl)0, (Rl)0);
+            });
+}
+
 // Even-length real inverse: bins 0..m (fewer if ic < m+1: missing bins read
 // as zero; imaginary parts of bins 0 and m ignored) are folded back into the
 // m-point packed spectrum Z, which is inverse transformed (conjugate trick)
 // and unpacked into 2m reals scaled by `scale`.  aux0 = W_2m^k table.
 struct OpC2RPacked {
+  static constexpr bool kConv = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    const int m = a.lp.n;
+    load_bins<P>(a, line0, m, m + 1, a.ic & 0x3fffffff);
+  }
+  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
     using C = typename P::cpx;
     using Rl = typename P::real;
     using TW = typename P::tw_t;
-    const C *in = (const C *)a.in.ptr;
     const TW *tw = (const TW *)a.aux0;
     const int m = a.lp.n;
-    const int nb = a.ic;  // bins available per line
     const int h = m / 2 + 1;
     const Rl half = (Rl)0.5;
-    const long long st = a.in.stride;
-    tile_loop(a.in, a.lpc, h, FastDiv((uint32_t)h), a.lpcdiv, line0, a.nlines,
-              [&](int l, int k, long long off) {
-                C *s = line_buf<P>(l, m);
-                const long long base = off - (long long)k * st;
-                auto bin = [&](int q) -> C {
-                  return q < nb ? in[base + (long long)q * st] : mkc((Rl)0, (Rl)0);
-                };
-                if (k == 0) {
-                  const Rl x0 = bin(0).x, xm = bin(m).x;
-                  // Z[0] = ((x0+xm) + i(x0-xm))/2, stored conjugated
-                  s[spad(0)] = mkc((x0 + xm) * half, -(x0 - xm) * half);
-                  return;
-                }
-                C xk = bin(k), xmk = bin(m - k);
-                // xe = (X[k] + conj X[m-k])/2 ; d = (X[k] - conj X[m-k])/2
-                C xe = mkc((xk.x + xmk.x) * half, (xk.y - xmk.y) * half);
-                C d = mkc((xk.x - xmk.x) * half, (xk.y + xmk.y) * half);
-                C xo = twmul(d, cconj_tw(__ldg(&tw[k])));
-                // Z[k] = xe + i xo ; Z[m-k] = conj(xe - i xo); store conjugates
-                C zk = mkc(xe.x - xo.y, xe.y + xo.x);
-                s[spad(k)] = cconj(zk);
-                if (m - k != k) {
-                  C zmk = mkc(xe.x + xo.y, -(xe.y - xo.x));
-                  s[spad(m - k)] = cconj(zmk);
-                }
-              });
+    const int total = a.lpc * h;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int l = e / h, k = e - l * h;
+      if (line0 + l >= a.nlines) continue;
+      C *s = line_buf<P>(l, m);
+      if (k == 0) {
+        const Rl x0 = s[spad(0)].x, xm = s[spad(m)].x;
+        // Z[0] = ((x0+xm) + i(x0-xm))/2, stored conjugated
+        s[spad(0)] = mkc((x0 + xm) * half, -(x0 - xm) * half);
+        continue;
+      }
+      C xk = s[spad(k)], xmk = s[spad(m - k)];
+      // xe = (X[k] + conj X[m-k])/2 ; d = (X[k] - conj X[m-k])/2
+      C xe = mkc((xk.x + xmk.x) * half, (xk.y - xmk.y) * half);
+      C d = mkc((xk.x - xmk.x) * half, (xk.y + xmk.y) * half);
+      C xo = twmul(d, cconj_tw(__ldg(&tw[k])));
+      // Z[k] = xe + i xo ; Z[m-k] = conj(xe - i xo); stored conjugated
+      s[spad(k)] = cconj(mkc(xe.x - xo.y, xe.y + xo.x));
+      if (m - k != k) s[spad(m - k)] = cconj(mkc(xe.x + xo.y, -(xe.y - xo.x)));
+    }
+    __syncthreads();
   }
   template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
     using C = typename P::cpx;
@@ -338,22 +417,25 @@ struct OpC2RPacked {
       out[base + st] = -y.y * sc;
     });
   }
-  static GF_DEV double2 cconj_tw(double2 w) { return make_double2(w.x, -w.y); }
-  static GF_DEV float2 cconj_tw(float2 w) { return make_float2(w.x, -w.y); }
-  static GF_DEV float4 cconj_tw(float4 w) { return make_float4(w.x, -w.y, w.z, -w.w); }
 };
 
 // Odd (or any) length real forward through a full complex line: reals are
-// promoted on load, the first n/2+1 bins are stored.
+// copied into the real parts, imaginary parts zeroed; the first n/2+1 bins
+// are stored.
 struct OpR2CFull {
+  static constexpr bool kConv = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
     using Rl = typename P::real;
     const Rl *in = (const Rl *)a.in.ptr;
     const int n = a.lp.n;
     tile_loop(a.in, a.lpc, n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      line_buf<P>(l, n)[spad(i)] = mkc(in[off], (Rl)0);
+      typename P::cpx *d = &line_buf<P>(l, n)[spad(i)];
+      cp_async_n<sizeof(Rl)>(&d->x, &in[off]);
+      d->y = (Rl)0;
     });
   }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
   template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
     using C = typename P::cpx;
     C *out = (C *)a.out.ptr;
@@ -368,26 +450,30 @@ struct OpR2CFull {
 // element i < n/2+1 is bin i, element i > n/2 is conj(bin(n-i)); bins at or
 // beyond ic read as zero.  Stored conjugated; the real part is the output.
 struct OpC2RFull {
+  static constexpr bool kConv = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    const int n = a.lp.n;
+    load_bins<P>(a, line0, n, n / 2 + 1, a.ic & 0x3fffffff);
+  }
+  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
     using C = typename P::cpx;
-    using Rl = typename P::real;
-    const C *in = (const C *)a.in.ptr;
     const int n = a.lp.n;
     const int h = n / 2 + 1;
-    const int nb = a.ic;
-    const long long st = a.in.stride;
-    tile_loop(a.in, a.lpc, n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      const long long base = off - (long long)i * st;
-      C v;
-      if (i < h) {
-        v = i < nb ? in[off] : mkc((Rl)0, (Rl)0);
-        v.y = -v.y;  // conjugate for the inverse
-      } else {
-        const int q = n - i;
-        v = q < nb ? in[base + (long long)q * st] : mkc((Rl)0, (Rl)0);  // conj(conj(bin))
-      }
-      line_buf<P>(l, n)[spad(i)] = v;
-    });
+    const int up = n - h;  // mirrored elements i = h .. n-1
+    for (int e = threadIdx.x; e < a.lpc * up; e += blockDim.x) {
+      const int l = e / up, i = h + (e - l * up);
+      C *s = line_buf<P>(l, n);
+      s[spad(i)] = s[spad(n - i)];  // conj(conj(bin(n-i)))
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < a.lpc * h; e += blockDim.x) {
+      const int l = e / h, i = e - l * h;
+      C *s = line_buf<P>(l, n);
+      s[spad(i)].y = -s[spad(i)].y;
+    }
+    __syncthreads();
+    (void)line0;
   }
   template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
     using Rl = typename P::real;

@@ -18,6 +18,7 @@ namespace gf {
 // ---------------------------------------------------------------------------
 struct OpRader {
   static constexpr bool kConv = true;
+  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
     using C = typename P::cpx;
     using Rl = typename P::real;
@@ -29,12 +30,9 @@ struct OpRader {
     const long long st = a.in.stride;
     tile_loop(a.in, a.lpc, cl, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int k, long long off) {
       const long long base = off - (long long)k * st;
-      C v = mkc((Rl)0, (Rl)0);
-      if (k < q) {
-        v = in[base + (long long)__ldg(&perm[k]) * st];
-        if (cj) v.y = -v.y;
-      }
-      line_buf<P>(l, cl)[spad(k)] = v;
+      C *d = &line_buf<P>(l, cl)[spad(k)];
+      if (k < q) cp_async_n<sizeof(C)>(d, &in[base + (long long)__ldg(&perm[k]) * st]);
+      else *d = mkc((Rl)0, (Rl)0);
       if (k == 0) {
         C x0 = in[base];
         if (cj) x0.y = -x0.y;
@@ -42,6 +40,7 @@ struct OpRader {
       }
     });
   }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
   template <class P> static GF_DEV void mid(const KArgs &a, long long line0) {
     using C = typename P::cpx;
     using SP = typename P::sp_t;
@@ -104,26 +103,36 @@ struct OpRader {
 // ---------------------------------------------------------------------------
 struct OpBluestein {
   static constexpr bool kConv = true;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
     using C = typename P::cpx;
     using Rl = typename P::real;
-    using SP = typename P::sp_t;
     const C *in = (const C *)a.in.ptr;
+    const int m = a.lp.n;
+    const int n = (int)a.ia;
+    tile_loop(a.in, a.lpc, m, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
+      C *d = &line_buf<P>(l, m)[spad(j)];
+      if (j < n) cp_async_n<sizeof(C)>(d, &in[off]);
+      else *d = mkc((Rl)0, (Rl)0);
+    });
+  }
+  // a[j] = conj?(x[j]) * w[j] for j < n
+  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
+    using C = typename P::cpx;
+    using SP = typename P::sp_t;
     const SP *w = (const SP *)a.aux0;
     const int m = a.lp.n;
     const int n = (int)a.ia;
     const bool cj = a.cj_in;
-    const long long st = a.in.stride;
-    tile_loop(a.in, a.lpc, m, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
-      C v = mkc((Rl)0, (Rl)0);
-      if (j < n) {
-        v = in[off];
-        if (cj) v.y = -v.y;
-        v = spmul(v, __ldg(&w[j]));
-      }
-      (void)st;
-      line_buf<P>(l, m)[spad(j)] = v;
-    });
+    for (int e = threadIdx.x; e < a.lpc * n; e += blockDim.x) {
+      const int l = e / n, j = e - l * n;
+      C *s = line_buf<P>(l, m);
+      C v = s[spad(j)];
+      if (cj) v.y = -v.y;
+      s[spad(j)] = spmul(v, __ldg(&w[j]));
+    }
+    __syncthreads();
+    (void)line0;
   }
   template <class P> static GF_DEV void mid(const KArgs &a, long long line0) {
     using C = typename P::cpx;
@@ -167,18 +176,28 @@ struct OpBluestein {
 // ---------------------------------------------------------------------------
 struct OpSpectro {
   static constexpr bool kConv = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    using Rl = typename P::real;
-    const Rl *in = (const Rl *)a.in.ptr;
-    const Rl *win = (const Rl *)a.aux1;
     const int m = a.lp.n;
     tile_loop(a.in, a.lpc, m, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
-      // stride 1: complex element j sits at off = line + j; its real pair is at
-      // line + 2j = off + j and off + j + 1
-      const Rl x0 = in[off + j] * __ldg(&win[2 * j]);
-      const Rl x1 = in[off + j + 1] * __ldg(&win[2 * j + 1]);
-      line_buf<P>(l, m)[spad(j)] = mkc(x0, x1);
+      // stride 1: complex element j sits at off = line + j; its real pair is
+      // at line + 2j = off + j
+      load_real_pair<P>(a, &line_buf<P>(l, m)[spad(j)], off + j, 1);
     });
+  }
+  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
+    using C = typename P::cpx;
+    using Rl = typename P::real;
+    const Rl *win = (const Rl *)a.aux1;
+    const int m = a.lp.n;
+    for (int e = threadIdx.x; e < a.lpc * m; e += blockDim.x) {
+      const int l = e / m, j = e - l * m;
+      C *s = line_buf<P>(l, m);
+      C v = s[spad(j)];
+      s[spad(j)] = mkc(v.x * __ldg(&win[2 * j]), v.y * __ldg(&win[2 * j + 1]));
+    }
+    __syncthreads();
+    (void)line0;
   }
   template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
     using C = typename P::cpx;
@@ -215,10 +234,6 @@ struct OpSpectro {
   }
 };
 
-template <class Op> struct ConvTrait { static constexpr bool v = false; };
-template <> struct ConvTrait<OpRader> { static constexpr bool v = true; };
-template <> struct ConvTrait<OpBluestein> { static constexpr bool v = true; };
-
 // ---------------------------------------------------------------------------
 // The line kernel: prologue, stages, [spectrum multiply, stages], epilogue.
 // ---------------------------------------------------------------------------
@@ -226,14 +241,16 @@ template <class P, int MAXE, class Op>
 __global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
   const long long line0 = (long long)blockIdx.x * a.lpc;
   Op::template load<P>(a, line0);
+  cp_async_wait_all();
   __syncthreads();
+  Op::template prep<P>(a, line0);
   const int l = threadIdx.x / a.lp.T;
   const int t = threadIdx.x - l * a.lp.T;
   typename P::cpx *s = line_buf<P>(l, a.lp.n);
-  run_stages<P, MAXE>(s, a.lp, t);
-  if constexpr (ConvTrait<Op>::v) {
+  run_stages<P, MAXE>(s, a.lp, t, Op::first_conj(a));
+  if constexpr (Op::kConv) {
     Op::template mid<P>(a, line0);
-    run_stages<P, MAXE>(s, a.lp, t);
+    run_stages<P, MAXE>(s, a.lp, t, false);
   }
   Op::template store<P>(a, line0);
 }

@@ -377,13 +377,15 @@ static int choose_lpc(const DevProg &dp, const KArgs &a, int op, long long nline
   const int colmode = (a.in.stride != 1 || a.out.stride != 1) ? 1 : 0;
   int lpc = get_lpc_override(dp.prec, dp.n, op, colmode);
   if (lpc <= 0) {
+    // about 256 threads and at most half the shared memory per CTA, so two
+    // CTAs share an SM: one's asynchronous prologue overlaps the other's
+    // butterflies
     lpc = std::max(1, 256 / T);
-    // keep two CTAs resident per SM where the lines allow it
-    while (lpc > 1 && (size_t)lpc * line_bytes > 100 * 1024) lpc--;
+    while (lpc > 1 && (size_t)lpc * line_bytes > smax / 2 - 1024) lpc--;
     if (colmode) {
-      // columns: enough adjacent lines per CTA to fill 128-byte segments
-      const int want = dp.prec == F64 ? 8 : 16;
-      int cap = (int)std::min<size_t>(512 / T, smax / line_bytes);
+      // columns: enough adjacent lines per CTA to fill 64-byte row segments
+      const int want = dp.prec == F64 ? 4 : 8;
+      const int cap = (int)std::min<size_t>(512 / T, smax / line_bytes);
       lpc = std::max(lpc, std::min(want, cap));
     }
   }
@@ -391,6 +393,14 @@ static int choose_lpc(const DevProg &dp, const KArgs &a, int op, long long nline
   while (lpc > 1 && (size_t)lpc * line_bytes > smax) lpc--;
   if (lpc > nlines) lpc = (int)std::max<long long>(1, nlines);
   return lpc;
+}
+
+// True when every real pair (x[2j], x[2j+1]) of every line of a real Side is
+// aligned to the pair size (so it moves as one vector copy).
+bool pairs_aligned(const Side &s, int prec) {
+  const long long pb = 2 * (long long)rsize(prec);
+  return s.stride == 1 && ((uintptr_t)s.ptr % pb) == 0 && (s.dist_b % 2) == 0 &&
+         (s.lpb.d == 1 || (s.dist_l % 2) == 0);
 }
 
 int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st, int lpc,
@@ -798,6 +808,7 @@ int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaS
       a.out = out;
       a.aux0 = tw2;
       a.scale = 1.0;
+      a.ic = pairs_aligned(in, prec) ? GF_PAIR_ALIGNED : 0;
       return launch_line(OP_R2C, *cx->prog, a, nl, st);
     }
     case R_FULL_FUSED: {

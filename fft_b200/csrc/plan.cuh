@@ -97,6 +97,7 @@ std::shared_ptr<DevProg> get_prog(long long n, int prec);
 std::shared_ptr<const Exec1D> get_exec(long long n, int prec);
 std::shared_ptr<const ExecReal> get_real(long long n, int prec);
 bool fits_single(long long n, int prec);
+bool pairs_aligned(const Side &s, int prec);
 
 // Launch helper for the line kernels.
 int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st,
