@@ -1,7 +1,7 @@
 // dispatch.h -- host-visible handles to the per-precision kernel instances.
 #pragma once
 #include <cuda_runtime.h>
-#include "engine.cuh"
+#include "ops.cuh"
 
 namespace gf {
 

@@ -1,4 +1,5 @@
-// engine.cuh -- the B200 line-FFT engine.
+// engine.cuh -- the B200 line-FFT engine: line programs, shared-memory
+// layout, the Stockham stage and the tile loops.
 //
 // A "line" is one 1-D transform of length n held entirely in one CTA's shared
 // memory.  A CTA processes `lpc` lines of the same length at once; `T` threads
@@ -9,19 +10,26 @@
 // output r to (j / Ns)*Ns*R + (j mod Ns) + r*Ns.  No digit-reversal pass is
 // needed; the last stage leaves natural order.
 //
-// Each stage is register-staged: every thread first loads all of its
-// butterflies' inputs from shared memory, the CTA synchronises, then each
-// thread computes and writes its outputs back over the same buffer.  One
-// buffer per line suffices, which doubles the longest single-CTA length.
-//
-// Global memory is touched only by the tile loops (prologue and epilogue):
-// the whole CTA cooperates over lpc x n elements, walking either along lines
-// (rows, unit stride) or across lines (columns of a row-major array), so both
-// sides are coalesced whatever the transform's axis.
+// Each stage is register-staged: every thread loads all of its butterflies'
+// inputs, the CTA synchronises, then each thread computes and writes its
+// outputs back over the same buffer (one buffer per line).  The first stage
+// can read its inputs straight from global memory and the last stage can
+// write straight to global memory ("direct" stages), so a transform of S
+// stages makes S-1 shared-memory round trips instead of S+1.  Direct stages
+// are coalesced because the thread mapping follows the layout: along a line
+// (row mode) or across adjacent lines (column mode, for axes that are not
+// contiguous).  Ops that need pairs of elements (real-signal packing) or a
+// gather the stage cannot express use the cooperative tile loops with
+// asynchronous copies instead.
 #pragma once
 #include "codelets.cuh"
 
 #define GF_MAXST 24
+
+// KArgs::flags
+#define GF_COLMAP 1        // thread mapping and smem layout across lines
+#define GF_FIRST_DIRECT 2  // first stage reads global memory
+#define GF_LAST_DIRECT 4   // last stage writes global memory
 
 namespace gf {
 
@@ -45,7 +53,7 @@ struct Side {
   FastDiv lpb;
 };
 
-GF_DEV long long line_off(const Side &s, uint32_t l) {
+GF_HD long long line_off(const Side &s, uint32_t l) {
   uint32_t b, r;
   s.lpb.divmod(l, b, r);
   return (long long)b * s.dist_b + (long long)r * s.dist_l;
@@ -64,7 +72,8 @@ struct KArgs {
   Side in, out;
   long long nlines;
   int lpc;           // lines per CTA
-  FastDiv ndiv;      // divide by the tile's row length (n, or bins for untangle)
+  int flags;         // GF_COLMAP | GF_FIRST_DIRECT | GF_LAST_DIRECT
+  FastDiv ndiv;      // divide by the line length n
   FastDiv lpcdiv;    // divide by lpc
   int cj_in;         // conjugate on load  (first pass of an inverse)
   int cj_out;        // conjugate on store (last pass of an inverse)
@@ -77,30 +86,101 @@ struct KArgs {
 };
 
 // ---------------------------------------------------------------------------
-// Stockham stage on shared memory.
+// Shared-memory layout of a CTA's lines.  Row mode: line-major, each line
+// padded (one spare element every 16).  Column mode: element-major with the
+// lpc lines interleaved, so consecutive threads (consecutive lines) touch
+// consecutive words.  A per-line view carries its base and element step.
 // ---------------------------------------------------------------------------
-template <class P, int R, int MAXE>
-GF_DEV void stage(typename P::cpx (&v)[MAXE], typename P::cpx *s, int n, int T, int ns,
-                  FastDiv nsd, const typename P::tw_t *tw, int t, bool cj) {
+template <class C> GF_DEV C *smem_base() {
+  extern __shared__ __align__(16) unsigned char g_smem[];
+  return reinterpret_cast<C *>(g_smem);
+}
+
+template <class C> struct LineView {
+  C *b;
+  int step;
+  GF_DEV C &operator[](int i) const { return b[spad(i) * step]; }
+};
+
+template <class C> GF_DEV LineView<C> line_view(const KArgs &a, int l) {
+  C *s = smem_base<C>();
+  LineView<C> v;
+  if (a.flags & GF_COLMAP) {
+    v.b = s + l;
+    v.step = a.lpc;
+  } else {
+    v.b = s + (size_t)l * spad_size(a.lp.n);
+    v.step = 1;
+  }
+  return v;
+}
+
+// Two spare complex slots per line after the lpc line buffers.
+template <class C> GF_DEV C *line_extra(const KArgs &a, int l) {
+  return smem_base<C>() + (size_t)a.lpc * spad_size(a.lp.n) + 2 * l;
+}
+
+// Per-thread context of a line kernel.
+struct LineCtx {
+  int l, t;              // local line, thread within the line
+  long long line;        // global line index
+  bool valid;            // line < nlines
+  long long ioff, ooff;  // element offsets of the line on the in / out sides
+};
+
+// ---------------------------------------------------------------------------
+// Asynchronous global -> shared copies (cp.async).
+// ---------------------------------------------------------------------------
+GF_DEV void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+GF_DEV void cp_async8(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+GF_DEV void cp_async4(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+GF_DEV void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+template <int BYTES> GF_DEV void cp_async_n(void *s, const void *g) {
+  if constexpr (BYTES == 16) cp_async16(s, g);
+  else if constexpr (BYTES == 8) cp_async8(s, g);
+  else cp_async4(s, g);
+}
+
+// ---------------------------------------------------------------------------
+// Stockham stage.  FG: inputs come from Op::gload (global memory) instead of
+// shared memory; TG: outputs go to Op::gstore instead of shared memory.
+// ---------------------------------------------------------------------------
+template <class P, class Op, int R, int MAXE, bool FG, bool TG>
+GF_DEV void stage(typename P::cpx (&v)[MAXE], const LineView<typename P::cpx> &s, const KArgs &a,
+                  const LineCtx &c, int ns, FastDiv nsd, const typename P::tw_t *tw, bool cj) {
   using C = typename P::cpx;
   constexpr int NB = MAXE / R;
+  const int n = a.lp.n, T = a.lp.T;
   const int nb = n / R;
 #pragma unroll
   for (int b = 0; b < NB; b++) {
-    const int j = t + b * T;
+    const int j = c.t + b * T;
     if (j < nb) {
 #pragma unroll
       for (int r = 0; r < R; r++) {
-        C x = s[spad(j + r * nb)];
+        C x;
+        if constexpr (FG) x = Op::template gload<P>(a, c, j + r * nb);
+        else x = s[j + r * nb];
         if (cj) x.y = -x.y;
         v[b * R + r] = x;
       }
     }
   }
-  __syncthreads();
+  if constexpr (!FG) __syncthreads();
 #pragma unroll
   for (int b = 0; b < NB; b++) {
-    const int j = t + b * T;
+    const int j = c.t + b * T;
     if (j < nb) {
       uint32_t q, k;
       nsd.divmod((uint32_t)j, q, k);
@@ -112,51 +192,91 @@ GF_DEV void stage(typename P::cpx (&v)[MAXE], typename P::cpx *s, int n, int T, 
       Dft<R, C>::run(&v[b * R]);
       const int base = (int)q * ns * R + (int)k;
 #pragma unroll
-      for (int r = 0; r < R; r++) s[spad(base + r * ns)] = v[b * R + r];
+      for (int r = 0; r < R; r++) {
+        if constexpr (TG) Op::template gstore<P>(a, c, base + r * ns, v[b * R + r]);
+        else s[base + r * ns] = v[b * R + r];
+      }
     }
   }
-  __syncthreads();
+  if constexpr (!TG) __syncthreads();
 }
 
-// Runs every stage of lp on the line buffer s.  All threads of the CTA call
+template <class P, class Op, int MAXE, bool FG, bool TG>
+GF_DEV void stage_sw(int R, typename P::cpx (&v)[MAXE], const LineView<typename P::cpx> &s,
+                     const KArgs &a, const LineCtx &c, int ns, FastDiv nsd,
+                     const typename P::tw_t *tw, bool cj) {
+  switch (R) {
+    case 2: stage<P, Op, 2, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    case 3: stage<P, Op, 3, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    case 4: stage<P, Op, 4, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    case 5: stage<P, Op, 5, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    case 7: stage<P, Op, 7, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    case 8: stage<P, Op, 8, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    case 11: stage<P, Op, 11, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    case 13: stage<P, Op, 13, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    case 16: stage<P, Op, 16, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    default: break;
+  }
+}
+
+// Runs every stage of lp on the line view s.  All threads of the CTA call
 // this (stages contain CTA barriers).  One register array serves every radix:
 // giving each radix case its own array makes ptxas allocate the switch
-// alternatives jointly and spill.  cj_first conjugates the inputs of the
-// first stage (or, for a stage-less line of length 1, the element itself).
-template <class P, int MAXE>
-GF_DEV void run_stages(typename P::cpx *s, const LineProg &lp, int t, bool cj_first) {
+// alternatives jointly and spill.  cj_first conjugates the first stage's
+// inputs.  first_g / last_g select the direct first / last stage (the op
+// must provide gload / gstore).
+template <class P, class Op, int MAXE, bool CAN_FG, bool CAN_TG>
+GF_DEV void run_stages(const LineView<typename P::cpx> &s, const KArgs &a, const LineCtx &c,
+                       bool cj_first, bool first_g, bool last_g) {
   using TW = typename P::tw_t;
   typename P::cpx v[MAXE];
-  const int n = lp.n, T = lp.T;
-  if (lp.nst == 0) {
-    if (cj_first && t == 0) s[0].y = -s[0].y;
+  const LineProg &lp = a.lp;
+  if (lp.nst == 0) {  // length-1 line: the transform is the identity
+    if (c.t == 0 && c.valid) {
+      typename P::cpx x;
+      if constexpr (CAN_FG) {
+        if (first_g) x = Op::template gload<P>(a, c, 0);
+        else x = s[0];
+      } else {
+        x = s[0];
+      }
+      if (cj_first) x.y = -x.y;
+      if constexpr (CAN_TG) {
+        if (last_g) Op::template gstore<P>(a, c, 0, x);
+        else s[0] = x;
+      } else {
+        s[0] = x;
+      }
+    }
     __syncthreads();
     return;
   }
   for (int si = 0; si < lp.nst; si++) {
+    const int R = lp.radix[si];
     const int ns = lp.ns[si];
     const FastDiv nsd = lp.nsdiv[si];
     const TW *tw = (const TW *)lp.tw + lp.twoff[si];
     const bool cj = cj_first && si == 0;
-    switch (lp.radix[si]) {
-      case 2: stage<P, 2, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
-      case 3: stage<P, 3, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
-      case 4: stage<P, 4, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
-      case 5: stage<P, 5, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
-      case 7: stage<P, 7, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
-      case 8: stage<P, 8, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
-      case 11: stage<P, 11, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
-      case 13: stage<P, 13, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
-      case 16: stage<P, 16, MAXE>(v, s, n, T, ns, nsd, tw, t, cj); break;
-      default: break;
+    const bool fg = first_g && si == 0;
+    const bool tg = last_g && si == lp.nst - 1;
+    if constexpr (CAN_FG && CAN_TG) {
+      if (fg && tg) { stage_sw<P, Op, MAXE, true, true>(R, v, s, a, c, ns, nsd, tw, cj); continue; }
     }
+    if constexpr (CAN_FG) {
+      if (fg) { stage_sw<P, Op, MAXE, true, false>(R, v, s, a, c, ns, nsd, tw, cj); continue; }
+    }
+    if constexpr (CAN_TG) {
+      if (tg) { stage_sw<P, Op, MAXE, false, true>(R, v, s, a, c, ns, nsd, tw, cj); continue; }
+    }
+    stage_sw<P, Op, MAXE, false, false>(R, v, s, a, c, ns, nsd, tw, cj);
   }
 }
 
 // ---------------------------------------------------------------------------
-// Tile loops.  f(l, i, off) is called for local line l, element i, with off the
-// element offset of (line, i) on the side.  Rows walk along lines; columns walk
-// across lines so consecutive threads touch consecutive lines.
+// Tile loops.  f(l, i, off) is called for local line l, element i (< len),
+// with off the element offset of (line, i) on the side.  Rows walk along
+// lines; columns walk across lines so consecutive threads touch consecutive
+// lines.
 // ---------------------------------------------------------------------------
 template <class F>
 GF_DEV void tile_loop(const Side &sd, int lpc, int len, FastDiv ldiv, FastDiv lpcdiv,
@@ -178,312 +298,5 @@ GF_DEV void tile_loop(const Side &sd, int lpc, int len, FastDiv ldiv, FastDiv lp
     }
   }
 }
-
-template <class P> GF_DEV typename P::cpx *line_buf(int l, int n) {
-  extern __shared__ __align__(16) unsigned char g_smem[];
-  return reinterpret_cast<typename P::cpx *>(g_smem) + (size_t)l * spad_size(n);
-}
-// Two spare complex slots per line after the lpc line buffers.
-template <class P> GF_DEV typename P::cpx *line_extra(int l, int n, int lpc) {
-  extern __shared__ __align__(16) unsigned char g_smem[];
-  return reinterpret_cast<typename P::cpx *>(g_smem) + (size_t)lpc * spad_size(n) + 2 * l;
-}
-
-// ---------------------------------------------------------------------------
-// Asynchronous global -> shared copies (cp.async): a tile's loads are all in
-// flight before any thread waits, so the prologue is bandwidth- rather than
-// latency-bound.  Data that needs arithmetic on arrival (conjugation, chirp,
-// window, real-spectrum folding) is copied raw and fixed up in shared memory.
-// ---------------------------------------------------------------------------
-GF_DEV void cp_async16(void *smem, const void *gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-GF_DEV void cp_async8(void *smem, const void *gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-GF_DEV void cp_async4(void *smem, const void *gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-GF_DEV void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-}
-// One element of `bytes` (4, 8 or 16).
-template <int BYTES> GF_DEV void cp_async_n(void *s, const void *g) {
-  if constexpr (BYTES == 16) cp_async16(s, g);
-  else if constexpr (BYTES == 8) cp_async8(s, g);
-  else cp_async4(s, g);
-}
-
-// KArgs::ic bit used by the real-input ops: real pairs are aligned to the
-// pair size, so a pair moves as one vector copy.
-#define GF_PAIR_ALIGNED 0x40000000
-
-// ---------------------------------------------------------------------------
-// Ops.  load() issues the prologue copies (completed by the kernel before
-// prep()); prep() runs in-shared-memory fix-ups and ends with a barrier when it
-// does anything; store() is the epilogue.  first_conj() asks the first Stockham
-// stage to conjugate what it reads (the inverse via conj(DFT(conj x))).
-// ---------------------------------------------------------------------------
-
-// Plain complex line: optional conjugation (inverse) and scale.
-struct OpC2C {
-  static constexpr bool kConv = false;
-  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    const C *in = (const C *)a.in.ptr;
-    const int n = a.lp.n;
-    tile_loop(a.in, a.lpc, n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      cp_async_n<sizeof(C)>(&line_buf<P>(l, n)[spad(i)], &in[off]);
-    });
-  }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    C *out = (C *)a.out.ptr;
-    const int n = a.lp.n;
-    const Rl sc = (Rl)a.scale;
-    const Rl sy = a.cj_out ? -sc : sc;
-    tile_loop(a.out, a.lpc, n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      C y = line_buf<P>(l, n)[spad(i)];
-      out[off] = mkc(y.x * sc, y.y * sy);
-    });
-  }
-};
-
-// Four-step pass 1 epilogue: element k1 of line n2 (line index within its
-// batch) is multiplied by W_N^{n2*k1} from the table aux0 (N entries).
-struct OpC2CTwiddle {
-  static constexpr bool kConv = false;
-  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    OpC2C::load<P>(a, line0);
-  }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using TW = typename P::tw_t;
-    C *out = (C *)a.out.ptr;
-    const TW *tw = (const TW *)a.aux0;
-    const int n = a.lp.n;
-    const long long NN = a.ia;  // full length N
-    tile_loop(a.out, a.lpc, n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      const uint32_t gl = (uint32_t)(line0 + l);
-      uint32_t b, n2;
-      a.out.lpb.divmod(gl, b, n2);
-      const long long e = ((long long)n2 * i) % NN;
-      C y = line_buf<P>(l, n)[spad(i)];
-      out[off] = twmul(y, __ldg(&tw[e]));
-    });
-  }
-};
-
-// Copies the real pair (x[2j], x[2j+1]) of a line into complex slot j.
-template <class P>
-GF_DEV void load_real_pair(const KArgs &a, typename P::cpx *dst, long long base, long long st) {
-  using Rl = typename P::real;
-  const Rl *in = (const Rl *)a.in.ptr;
-  if (a.ic & GF_PAIR_ALIGNED) {
-    cp_async_n<2 * sizeof(Rl)>(dst, &in[base]);
-  } else {
-    cp_async_n<sizeof(Rl)>(&dst->x, &in[base]);
-    cp_async_n<sizeof(Rl)>(&dst->y, &in[base + st]);
-  }
-}
-
-// Even-length real forward: the 2m reals of a line are read as m complex
-// values z[j] = x[2j] + i x[2j+1]; after the m-point FFT the untangle
-//   X[k] = (Z[k] + conj Z[m-k])/2 + W_2m^k (Z[k] - conj Z[m-k])/(2i)
-// writes bins 0..m (aux0 = W_2m^k table, k = 0..m).  Sides count reals on
-// input and complex bins on output.
-struct OpR2CPacked {
-  static constexpr bool kConv = false;
-  static GF_DEV bool first_conj(const KArgs &) { return false; }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    const int m = a.lp.n;
-    const long long st = a.in.stride;
-    tile_loop(a.in, a.lpc, m, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
-      // off addresses element j with stride st; the real pair is at 2j, 2j+1
-      const long long base = off - (long long)j * st + 2LL * j * st;
-      load_real_pair<P>(a, &line_buf<P>(l, m)[spad(j)], base, st);
-    });
-  }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    using TW = typename P::tw_t;
-    C *out = (C *)a.out.ptr;
-    const TW *tw = (const TW *)a.aux0;
-    const int m = a.lp.n;
-    const int h = m / 2 + 1;  // pair index k = 0..m/2
-    const Rl half = (Rl)0.5;
-    const long long st = a.out.stride;
-    tile_loop(a.out, a.lpc, h, FastDiv((uint32_t)h), a.lpcdiv, line0, a.nlines,
-              [&](int l, int k, long long off) {
-                const C *s = line_buf<P>(l, m);
-                const long long base = off - (long long)k * st;
-                if (k == 0) {
-                  C z0 = s[spad(0)];
-                  out[base] = mkc(z0.x + z0.y, (Rl)0);
-                  out[base + (long long)m * st] = mkc(z0.x - z0.y, (Rl)0);
-                  return;
-                }
-                C zk = s[spad(k)], zm = s[spad(m - k)];
-                C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
-                C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
-                C t = twmul(xo, __ldg(&tw[k]));
-                out[off] = cadd(xe, t);
-                if (m - k != k) out[base + (long long)(m - k) * st] = mkc(xe.x - t.x, t.y - xe.y);
-              });
-  }
-};
-
-GF_DEV double2 cconj_tw(double2 w) { return make_double2(w.x, -w.y); }
-GF_DEV float2 cconj_tw(float2 w) { return make_float2(w.x, -w.y); }
-GF_DEV float4 cconj_tw(float4 w) { return make_float4(w.x, -w.y, w.z, -w.w); }
-
-// Copies bins 0..min(nb, cnt)-1 of each line raw into slots 0.., zeroing the
-// slots of missing bins up to cnt.
-template <class P>
-GF_DEV void load_bins(const KArgs &a, long long line0, int slots, int cnt, int nb) {
-  using C = typename P::cpx;
-  using Rl = typename P::real;
-  const C *in = (const C *)a.in.ptr;
-  tile_loop(a.in, a.lpc, cnt, FastDiv((uint32_t)cnt), a.lpcdiv, line0, a.nlines,
-            [&](int l, int k, long long off) {
-              C *d = &line_buf<P>(l, slots)[spad(k)];
-              if (k < nb) cp_async_n<sizeof(C)>(d, &in[off]);
-              else *d = mkc((Rl)0, (Rl)0);
-            });
-}
-
-// Even-length real inverse: bins 0..m (fewer if ic < m+1: missing bins read
-// as zero; imaginary parts of bins 0 and m ignored) are folded back into the
-// m-point packed spectrum Z, which is inverse transformed (conjugate trick)
-// and unpacked into 2m reals scaled by `scale`.  aux0 = W_2m^k table.
-struct OpC2RPacked {
-  static constexpr bool kConv = false;
-  static GF_DEV bool first_conj(const KArgs &) { return false; }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    const int m = a.lp.n;
-    load_bins<P>(a, line0, m, m + 1, a.ic & 0x3fffffff);
-  }
-  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    using TW = typename P::tw_t;
-    const TW *tw = (const TW *)a.aux0;
-    const int m = a.lp.n;
-    const int h = m / 2 + 1;
-    const Rl half = (Rl)0.5;
-    const int total = a.lpc * h;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int l = e / h, k = e - l * h;
-      if (line0 + l >= a.nlines) continue;
-      C *s = line_buf<P>(l, m);
-      if (k == 0) {
-        const Rl x0 = s[spad(0)].x, xm = s[spad(m)].x;
-        // Z[0] = ((x0+xm) + i(x0-xm))/2, stored conjugated
-        s[spad(0)] = mkc((x0 + xm) * half, -(x0 - xm) * half);
-        continue;
-      }
-      C xk = s[spad(k)], xmk = s[spad(m - k)];
-      // xe = (X[k] + conj X[m-k])/2 ; d = (X[k] - conj X[m-k])/2
-      C xe = mkc((xk.x + xmk.x) * half, (xk.y - xmk.y) * half);
-      C d = mkc((xk.x - xmk.x) * half, (xk.y + xmk.y) * half);
-      C xo = twmul(d, cconj_tw(__ldg(&tw[k])));
-      // Z[k] = xe + i xo ; Z[m-k] = conj(xe - i xo); stored conjugated
-      s[spad(k)] = cconj(mkc(xe.x - xo.y, xe.y + xo.x));
-      if (m - k != k) s[spad(m - k)] = cconj(mkc(xe.x + xo.y, -(xe.y - xo.x)));
-    }
-    __syncthreads();
-  }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    Rl *out = (Rl *)a.out.ptr;
-    const int m = a.lp.n;
-    const Rl sc = (Rl)a.scale;
-    const long long st = a.out.stride;
-    tile_loop(a.out, a.lpc, m, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
-      C y = line_buf<P>(l, m)[spad(j)];
-      const long long base = off - (long long)j * st + 2LL * j * st;
-      out[base] = y.x * sc;
-      out[base + st] = -y.y * sc;
-    });
-  }
-};
-
-// Odd (or any) length real forward through a full complex line: reals are
-// copied into the real parts, imaginary parts zeroed; the first n/2+1 bins
-// are stored.
-struct OpR2CFull {
-  static constexpr bool kConv = false;
-  static GF_DEV bool first_conj(const KArgs &) { return false; }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    using Rl = typename P::real;
-    const Rl *in = (const Rl *)a.in.ptr;
-    const int n = a.lp.n;
-    tile_loop(a.in, a.lpc, n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      typename P::cpx *d = &line_buf<P>(l, n)[spad(i)];
-      cp_async_n<sizeof(Rl)>(&d->x, &in[off]);
-      d->y = (Rl)0;
-    });
-  }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    C *out = (C *)a.out.ptr;
-    const int n = a.lp.n;
-    const int h = n / 2 + 1;
-    tile_loop(a.out, a.lpc, h, FastDiv((uint32_t)h), a.lpcdiv, line0, a.nlines,
-              [&](int l, int k, long long off) { out[off] = line_buf<P>(l, n)[spad(k)]; });
-  }
-};
-
-// Odd (or any) length real inverse through the full Hermitian mirror:
-// element i < n/2+1 is bin i, element i > n/2 is conj(bin(n-i)); bins at or
-// beyond ic read as zero.  Stored conjugated; the real part is the output.
-struct OpC2RFull {
-  static constexpr bool kConv = false;
-  static GF_DEV bool first_conj(const KArgs &) { return false; }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    const int n = a.lp.n;
-    load_bins<P>(a, line0, n, n / 2 + 1, a.ic & 0x3fffffff);
-  }
-  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    const int n = a.lp.n;
-    const int h = n / 2 + 1;
-    const int up = n - h;  // mirrored elements i = h .. n-1
-    for (int e = threadIdx.x; e < a.lpc * up; e += blockDim.x) {
-      const int l = e / up, i = h + (e - l * up);
-      C *s = line_buf<P>(l, n);
-      s[spad(i)] = s[spad(n - i)];  // conj(conj(bin(n-i)))
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < a.lpc * h; e += blockDim.x) {
-      const int l = e / h, i = e - l * h;
-      C *s = line_buf<P>(l, n);
-      s[spad(i)].y = -s[spad(i)].y;
-    }
-    __syncthreads();
-    (void)line0;
-  }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
-    using Rl = typename P::real;
-    Rl *out = (Rl *)a.out.ptr;
-    const int n = a.lp.n;
-    const Rl sc = (Rl)a.scale;
-    tile_loop(a.out, a.lpc, n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      out[off] = line_buf<P>(l, n)[spad(i)].x * sc;
-    });
-  }
-};
 
 }  // namespace gf

@@ -1,258 +1,50 @@
-// kernels.cuh -- fused convolution ops (Rader, Bluestein), the spectrogram
-// op, the line kernel itself, and the elementwise kernels used by multi-pass
-// plans and plan construction (twiddle, chirp and permutation tables).
+// kernels.cuh -- the line kernel, and the elementwise kernels used by
+// multi-pass plans and plan construction (twiddle and spectrum tables).
 #pragma once
 #include <type_traits>
-#include "engine.cuh"
+#include "ops.cuh"
 
 namespace gf {
 
 // ---------------------------------------------------------------------------
-// Rader, fused in one CTA (rader.go:129-172 restated for one line):
-//   a[k] = x[perm[k]] (k < q = p-1, zero-padded to cl), A = FFT_cl(a),
-//   X[0] = x0 + A[0] (= sum of all inputs),
-//   conv = IFFT_cl(A * B)  evaluated as conj(FFT_cl(conj(A * B / cl))),
-//   X[iperm[qi]] = x0 + conv[qi + off]   (off = 0 cyclic, q padded-linear).
-// aux0 = perm (int32, q), aux1 = iperm (int32, q), aux2 = B/cl (sp_t, cl),
-// ia = p, ic = off.  lp is the length-cl program.
-// ---------------------------------------------------------------------------
-struct OpRader {
-  static constexpr bool kConv = true;
-  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    const C *in = (const C *)a.in.ptr;
-    const int *perm = (const int *)a.aux0;
-    const int cl = a.lp.n;
-    const int q = (int)a.ia - 1;
-    const bool cj = a.cj_in;
-    const long long st = a.in.stride;
-    tile_loop(a.in, a.lpc, cl, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int k, long long off) {
-      const long long base = off - (long long)k * st;
-      C *d = &line_buf<P>(l, cl)[spad(k)];
-      if (k < q) cp_async_n<sizeof(C)>(d, &in[base + (long long)__ldg(&perm[k]) * st]);
-      else *d = mkc((Rl)0, (Rl)0);
-      if (k == 0) {
-        C x0 = in[base];
-        if (cj) x0.y = -x0.y;
-        line_extra<P>(l, cl, a.lpc)[0] = x0;
-      }
-    });
-  }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void mid(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using SP = typename P::sp_t;
-    const SP *B = (const SP *)a.aux2;
-    const int cl = a.lp.n;
-    // DC first (reads A[0] before the multiply overwrites it)
-    for (int l = threadIdx.x; l < a.lpc; l += blockDim.x) {
-      C *ex = line_extra<P>(l, cl, a.lpc);
-      ex[1] = cadd(ex[0], line_buf<P>(l, cl)[spad(0)]);
-    }
-    __syncthreads();
-    const int total = a.lpc * cl;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      uint32_t l, k;
-      a.ndiv.divmod((uint32_t)e, l, k);
-      C *s = line_buf<P>((int)l, cl);
-      s[spad(k)] = cconj(spmul(s[spad(k)], __ldg(&B[k])));
-    }
-    __syncthreads();
-  }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    C *out = (C *)a.out.ptr;
-    const int *iperm = (const int *)a.aux1;
-    const int cl = a.lp.n;
-    const int p = (int)a.ia;
-    const int q = p - 1;
-    const int offc = a.ic;
-    const Rl sc = (Rl)a.scale;
-    const Rl sy = a.cj_out ? -sc : sc;
-    const long long st = a.out.stride;
-    tile_loop(a.out, a.lpc, p, FastDiv((uint32_t)p), a.lpcdiv, line0, a.nlines,
-              [&](int l, int i, long long off) {
-                const long long base = off - (long long)i * st;
-                const C *ex = line_extra<P>(l, cl, a.lpc);
-                C y;
-                long long dst;
-                if (i == 0) {
-                  y = ex[1];
-                  dst = 0;
-                } else {
-                  const int qi = i - 1;
-                  C c = cconj(line_buf<P>(l, cl)[spad(qi + offc)]);
-                  y = cadd(ex[0], c);
-                  dst = __ldg(&iperm[qi]);
-                }
-                (void)q;
-                out[base + dst * st] = mkc(y.x * sc, y.y * sy);
-              });
-  }
-};
-
-// ---------------------------------------------------------------------------
-// Bluestein, fused in one CTA (bluestein.go:67-95 restated for one line):
-//   a[j] = x[j] w[j] (j < n, zero-padded to m), conv = IFFT_m(FFT_m(a) * B)
-//   with B = FFT_m(b) / m, evaluated as conj(FFT_m(conj(FFT_m(a) * B))),
-//   X[k] = conv[k] w[k].
-// aux0 = chirp w (sp_t, n), aux2 = B/m (sp_t, m), ia = n.  lp has length m.
-// ---------------------------------------------------------------------------
-struct OpBluestein {
-  static constexpr bool kConv = true;
-  static GF_DEV bool first_conj(const KArgs &) { return false; }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    const C *in = (const C *)a.in.ptr;
-    const int m = a.lp.n;
-    const int n = (int)a.ia;
-    tile_loop(a.in, a.lpc, m, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
-      C *d = &line_buf<P>(l, m)[spad(j)];
-      if (j < n) cp_async_n<sizeof(C)>(d, &in[off]);
-      else *d = mkc((Rl)0, (Rl)0);
-    });
-  }
-  // a[j] = conj?(x[j]) * w[j] for j < n
-  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using SP = typename P::sp_t;
-    const SP *w = (const SP *)a.aux0;
-    const int m = a.lp.n;
-    const int n = (int)a.ia;
-    const bool cj = a.cj_in;
-    for (int e = threadIdx.x; e < a.lpc * n; e += blockDim.x) {
-      const int l = e / n, j = e - l * n;
-      C *s = line_buf<P>(l, m);
-      C v = s[spad(j)];
-      if (cj) v.y = -v.y;
-      s[spad(j)] = spmul(v, __ldg(&w[j]));
-    }
-    __syncthreads();
-    (void)line0;
-  }
-  template <class P> static GF_DEV void mid(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using SP = typename P::sp_t;
-    const SP *B = (const SP *)a.aux2;
-    const int m = a.lp.n;
-    const int total = a.lpc * m;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      uint32_t l, k;
-      a.ndiv.divmod((uint32_t)e, l, k);
-      C *s = line_buf<P>((int)l, m);
-      s[spad(k)] = cconj(spmul(s[spad(k)], __ldg(&B[k])));
-    }
-    __syncthreads();
-  }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    using SP = typename P::sp_t;
-    C *out = (C *)a.out.ptr;
-    const SP *w = (const SP *)a.aux0;
-    const int m = a.lp.n;
-    const int n = (int)a.ia;
-    const Rl sc = (Rl)a.scale;
-    const Rl sy = a.cj_out ? -sc : sc;
-    tile_loop(a.out, a.lpc, n, FastDiv((uint32_t)n), a.lpcdiv, line0, a.nlines,
-              [&](int l, int k, long long off) {
-                C y = spmul(cconj(line_buf<P>(l, m)[spad(k)]), __ldg(&w[k]));
-                out[off] = mkc(y.x * sc, y.y * sy);
-              });
-  }
-};
-
-// ---------------------------------------------------------------------------
-// Spectrogram frame (freq.go:107-127 with PSD freq.go:69-90): line t is the
-// frame x[t*step .. t*step+seg) times the window, transformed as an even
-// real line (seg = 2m) and reduced to the one-sided density
-//   p[k] = |X[k]|^2 * scale, doubled except for k = 0 and k = m.
-// in: real signal (Side: dist_b = step per frame, stride 1); aux1 = window
-// (real, seg); aux0 = W_2m^k table; out: real bins (m+1 per frame).
-// ---------------------------------------------------------------------------
-struct OpSpectro {
-  static constexpr bool kConv = false;
-  static GF_DEV bool first_conj(const KArgs &) { return false; }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    const int m = a.lp.n;
-    tile_loop(a.in, a.lpc, m, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
-      // stride 1: complex element j sits at off = line + j; its real pair is
-      // at line + 2j = off + j
-      load_real_pair<P>(a, &line_buf<P>(l, m)[spad(j)], off + j, 1);
-    });
-  }
-  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    const Rl *win = (const Rl *)a.aux1;
-    const int m = a.lp.n;
-    for (int e = threadIdx.x; e < a.lpc * m; e += blockDim.x) {
-      const int l = e / m, j = e - l * m;
-      C *s = line_buf<P>(l, m);
-      C v = s[spad(j)];
-      s[spad(j)] = mkc(v.x * __ldg(&win[2 * j]), v.y * __ldg(&win[2 * j + 1]));
-    }
-    __syncthreads();
-    (void)line0;
-  }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
-    using C = typename P::cpx;
-    using Rl = typename P::real;
-    using TW = typename P::tw_t;
-    Rl *out = (Rl *)a.out.ptr;
-    const TW *tw = (const TW *)a.aux0;
-    const int m = a.lp.n;
-    const int h = m / 2 + 1;
-    const Rl half = (Rl)0.5;
-    const Rl sc = (Rl)a.scale;
-    tile_loop(a.out, a.lpc, h, FastDiv((uint32_t)h), a.lpcdiv, line0, a.nlines,
-              [&](int l, int k, long long off) {
-                const C *s = line_buf<P>(l, m);
-                const long long base = off - k;
-                if (k == 0) {
-                  C z0 = s[spad(0)];
-                  const Rl d0 = z0.x + z0.y, dm = z0.x - z0.y;
-                  out[base] = d0 * d0 * sc;
-                  out[base + m] = dm * dm * sc;
-                  return;
-                }
-                C zk = s[spad(k)], zm = s[spad(m - k)];
-                C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
-                C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
-                C t = twmul(xo, __ldg(&tw[k]));
-                C xk = cadd(xe, t);
-                out[off] = (xk.x * xk.x + xk.y * xk.y) * sc * (Rl)2;
-                if (m - k != k) {
-                  C xm = csub(xe, t);
-                  out[base + (m - k)] = (xm.x * xm.x + xm.y * xm.y) * sc * (Rl)2;
-                }
-              });
-  }
-};
-
-// ---------------------------------------------------------------------------
-// The line kernel: prologue, stages, [spectrum multiply, stages], epilogue.
+// The line kernel: [tile prologue], stages, [spectrum multiply, stages],
+// [tile epilogue].  Threads map along lines (row mode) or across lines
+// (GF_COLMAP); the first / last stage read / write global memory directly
+// when the op supports it and the host set GF_FIRST_DIRECT / GF_LAST_DIRECT.
 // ---------------------------------------------------------------------------
 template <class P, int MAXE, class Op>
 __global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
+  using C = typename P::cpx;
   const long long line0 = (long long)blockIdx.x * a.lpc;
-  Op::template load<P>(a, line0);
-  cp_async_wait_all();
-  __syncthreads();
-  Op::template prep<P>(a, line0);
-  const int l = threadIdx.x / a.lp.T;
-  const int t = threadIdx.x - l * a.lp.T;
-  typename P::cpx *s = line_buf<P>(l, a.lp.n);
-  run_stages<P, MAXE>(s, a.lp, t, Op::first_conj(a));
-  if constexpr (Op::kConv) {
-    Op::template mid<P>(a, line0);
-    run_stages<P, MAXE>(s, a.lp, t, false);
+  LineCtx c;
+  if (a.flags & GF_COLMAP) {
+    c.l = threadIdx.x % a.lpc;
+    c.t = threadIdx.x / a.lpc;
+  } else {
+    c.l = threadIdx.x / a.lp.T;
+    c.t = threadIdx.x - c.l * a.lp.T;
   }
-  Op::template store<P>(a, line0);
+  c.line = line0 + c.l;
+  c.valid = c.line < a.nlines;
+  c.ioff = c.valid ? line_off(a.in, (uint32_t)c.line) : 0;
+  c.ooff = c.valid ? line_off(a.out, (uint32_t)c.line) : 0;
+  const bool first_g = Op::kFG && (a.flags & GF_FIRST_DIRECT);
+  const bool last_g = Op::kTG && (a.flags & GF_LAST_DIRECT);
+  if (!first_g) {
+    Op::template load<P>(a, line0);
+    cp_async_wait_all();
+    __syncthreads();
+    Op::template prep<P>(a, line0);
+  }
+  const LineView<C> s = line_view<C>(a, c.l);
+  if constexpr (Op::kConv) {
+    run_stages<P, Op, MAXE, Op::kFG, false>(s, a, c, Op::first_conj(a), first_g, false);
+    Op::template mid<P>(a, line0, last_g);
+    run_stages<P, Op, MAXE, false, Op::kTG>(s, a, c, false, false, last_g);
+  } else {
+    run_stages<P, Op, MAXE, Op::kFG, Op::kTG>(s, a, c, Op::first_conj(a), first_g, last_g);
+  }
+  if (!last_g) Op::template store<P>(a, line0);
 }
 
 // ===========================================================================

@@ -1,0 +1,586 @@
+// ops.cuh -- what a line kernel reads and writes around the Stockham stages.
+//
+// Each op provides some of:
+//   gload(a, c, i)      element i of the line's input (direct first stage)
+//   gstore(a, c, i, v)  element i of the line's output (direct last stage)
+//   load / prep         tile prologue: asynchronous copies into shared memory
+//                       and in-shared-memory fix-ups (when the first stage is
+//                       not direct, or the op needs element pairs)
+//   store               tile epilogue (when the last stage is not direct)
+//   mid                 convolution ops: spectrum multiply between the two FFTs
+// kFG / kTG say whether gload / gstore exist; first_conj(a) asks the first
+// stage to conjugate its inputs (inverse transforms as conj(DFT(conj x))).
+#pragma once
+#include "engine.cuh"
+
+// KArgs::ic bit used by the real-input ops: real pairs are aligned to the
+// pair size, so a pair moves as one vector access.
+#define GF_PAIR_ALIGNED 0x40000000
+#define GF_IC_MASK 0x3fffffff
+
+namespace gf {
+
+template <class P> using Cx = typename P::cpx;
+
+GF_DEV double2 cconj_tw(double2 w) { return make_double2(w.x, -w.y); }
+GF_DEV float2 cconj_tw(float2 w) { return make_float2(w.x, -w.y); }
+GF_DEV float4 cconj_tw(float4 w) { return make_float4(w.x, -w.y, w.z, -w.w); }
+
+// Reads the real pair (x[base], x[base + st]) as one complex value.
+template <class P> GF_DEV Cx<P> read_pair(const KArgs &a, long long base, long long st) {
+  using Rl = typename P::real;
+  const Rl *in = (const Rl *)a.in.ptr;
+  if (a.ic & GF_PAIR_ALIGNED) return *reinterpret_cast<const Cx<P> *>(&in[base]);
+  return mkc(in[base], in[base + st]);
+}
+
+// Copies the real pair (x[base], x[base + st]) into a complex slot.
+template <class P> GF_DEV void load_real_pair(const KArgs &a, Cx<P> *dst, long long base, long long st) {
+  using Rl = typename P::real;
+  const Rl *in = (const Rl *)a.in.ptr;
+  if (a.ic & GF_PAIR_ALIGNED) {
+    cp_async_n<2 * sizeof(Rl)>(dst, &in[base]);
+  } else {
+    cp_async_n<sizeof(Rl)>(&dst->x, &in[base]);
+    cp_async_n<sizeof(Rl)>(&dst->y, &in[base + st]);
+  }
+}
+
+// Copies bins 0..min(nb, cnt)-1 of each line raw into slots 0.., zeroing the
+// slots of missing bins up to cnt.
+template <class P> GF_DEV void load_bins(const KArgs &a, long long line0, int cnt, int nb) {
+  using C = Cx<P>;
+  using Rl = typename P::real;
+  const C *in = (const C *)a.in.ptr;
+  tile_loop(a.in, a.lpc, cnt, FastDiv((uint32_t)cnt), a.lpcdiv, line0, a.nlines,
+            [&](int l, int k, long long off) {
+              C *d = &line_view<C>(a, l)[k];
+              if (k < nb) cp_async_n<sizeof(C)>(d, &in[off]);
+              else *d = mkc((Rl)0, (Rl)0);
+            });
+}
+
+// ---------------------------------------------------------------------------
+// Plain complex line: optional conjugation (inverse) and scale.
+// ---------------------------------------------------------------------------
+struct OpC2C {
+  static constexpr bool kConv = false, kFG = true, kTG = true;
+  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int i) {
+    using Rl = typename P::real;
+    if (!c.valid) return mkc((Rl)0, (Rl)0);
+    return ((const Cx<P> *)a.in.ptr)[c.ioff + (long long)i * a.in.stride];
+  }
+  template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
+    using Rl = typename P::real;
+    if (!c.valid) return;
+    const Rl sc = (Rl)a.scale;
+    ((Cx<P> *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = mkc(y.x * sc, y.y * (a.cj_out ? -sc : sc));
+  }
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    const C *in = (const C *)a.in.ptr;
+    tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
+      cp_async_n<sizeof(C)>(&line_view<C>(a, l)[i], &in[off]);
+    });
+  }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    C *out = (C *)a.out.ptr;
+    const Rl sc = (Rl)a.scale;
+    const Rl sy = a.cj_out ? -sc : sc;
+    tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
+      C y = line_view<C>(a, l)[i];
+      out[off] = mkc(y.x * sc, y.y * sy);
+    });
+  }
+};
+
+// Four-step pass 1: element k1 of line n2 (the line's index within its batch)
+// is multiplied by W_N^{n2*k1} from the table aux0 (N = ia entries).
+struct OpC2CTwiddle {
+  static constexpr bool kConv = false, kFG = true, kTG = true;
+  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int i) {
+    return OpC2C::gload<P>(a, c, i);
+  }
+  template <class P> static GF_DEV Cx<P> tw(const KArgs &a, long long line, int i, Cx<P> y) {
+    using TW = typename P::tw_t;
+    uint32_t b, n2;
+    a.out.lpb.divmod((uint32_t)line, b, n2);
+    const long long e = ((long long)n2 * i) % a.ia;
+    return twmul(y, __ldg(&((const TW *)a.aux0)[e]));
+  }
+  template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
+    if (!c.valid) return;
+    ((Cx<P> *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = tw<P>(a, c.line, i, y);
+  }
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0) { OpC2C::load<P>(a, line0); }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    C *out = (C *)a.out.ptr;
+    tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
+      out[off] = tw<P>(a, line0 + l, i, line_view<C>(a, l)[i]);
+    });
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Even-length real forward: the 2m reals of a line are read as m complex
+// values z[j] = x[2j] + i x[2j+1]; after the m-point FFT the untangle
+//   X[k] = (Z[k] + conj Z[m-k])/2 + W_2m^k (Z[k] - conj Z[m-k])/(2i)
+// writes bins 0..m (aux0 = W_2m^k table, k = 0..m).  Sides count reals on
+// input and complex bins on output.
+// ---------------------------------------------------------------------------
+template <class P, class F>
+GF_DEV void untangle_tile(const KArgs &a, long long line0, F emit) {
+  using C = Cx<P>;
+  using Rl = typename P::real;
+  using TW = typename P::tw_t;
+  const TW *tw = (const TW *)a.aux0;
+  const int m = a.lp.n;
+  const int h = m / 2 + 1;  // pair index k = 0..m/2
+  const Rl half = (Rl)0.5;
+  tile_loop(a.out, a.lpc, h, FastDiv((uint32_t)h), a.lpcdiv, line0, a.nlines,
+            [&](int l, int k, long long off) {
+              const LineView<C> s = line_view<C>(a, l);
+              const long long base = off - (long long)k * a.out.stride;
+              if (k == 0) {
+                C z0 = s[0];
+                emit(base, 0, mkc(z0.x + z0.y, (Rl)0));
+                emit(base, m, mkc(z0.x - z0.y, (Rl)0));
+                return;
+              }
+              C zk = s[k], zm = s[m - k];
+              C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
+              C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
+              C t = twmul(xo, __ldg(&tw[k]));
+              emit(base, k, cadd(xe, t));
+              if (m - k != k) emit(base, m - k, mkc(xe.x - t.x, t.y - xe.y));
+            });
+}
+
+struct OpR2CPacked {
+  static constexpr bool kConv = false, kFG = true, kTG = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int j) {
+    using Rl = typename P::real;
+    if (!c.valid) return mkc((Rl)0, (Rl)0);
+    return read_pair<P>(a, c.ioff + 2LL * j * a.in.stride, a.in.stride);
+  }
+  template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    const long long st = a.in.stride;
+    tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
+      const long long base = off - (long long)j * st + 2LL * j * st;
+      load_real_pair<P>(a, &line_view<Cx<P>>(a, l)[j], base, st);
+    });
+  }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+    Cx<P> *out = (Cx<P> *)a.out.ptr;
+    const long long st = a.out.stride;
+    untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) { out[base + (long long)k * st] = v; });
+  }
+};
+
+// Even-length real inverse: bins 0..m (fewer if ic < m+1: missing bins read
+// as zero; imaginary parts of bins 0 and m ignored) are folded back into the
+// m-point packed spectrum Z, which is inverse transformed (conjugate trick)
+// and unpacked into 2m reals scaled by `scale`.  aux0 = W_2m^k table.
+struct OpC2RPacked {
+  static constexpr bool kConv = false, kFG = false, kTG = true;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &, const LineCtx &, int) { return Cx<P>(); }
+  template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int j, Cx<P> y) {
+    using Rl = typename P::real;
+    if (!c.valid) return;
+    Rl *out = (Rl *)a.out.ptr;
+    const Rl sc = (Rl)a.scale;
+    const long long st = a.out.stride;
+    const long long base = c.ooff + 2LL * j * st;
+    if (a.ic & GF_PAIR_ALIGNED) {
+      *reinterpret_cast<Cx<P> *>(&out[base]) = mkc(y.x * sc, -y.y * sc);
+    } else {
+      out[base] = y.x * sc;
+      out[base + st] = -y.y * sc;
+    }
+  }
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    const int m = a.lp.n;
+    load_bins<P>(a, line0, m + 1, a.ic & GF_IC_MASK);
+  }
+  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    using TW = typename P::tw_t;
+    const TW *tw = (const TW *)a.aux0;
+    const int m = a.lp.n;
+    const int h = m / 2 + 1;
+    const Rl half = (Rl)0.5;
+    const int total = a.lpc * h;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int l = e / h, k = e - l * h;
+      if (line0 + l >= a.nlines) continue;
+      const LineView<C> s = line_view<C>(a, l);
+      if (k == 0) {
+        const Rl x0 = s[0].x, xm = s[m].x;
+        // Z[0] = ((x0+xm) + i(x0-xm))/2, stored conjugated
+        s[0] = mkc((x0 + xm) * half, -(x0 - xm) * half);
+        continue;
+      }
+      C xk = s[k], xmk = s[m - k];
+      // xe = (X[k] + conj X[m-k])/2 ; d = (X[k] - conj X[m-k])/2
+      C xe = mkc((xk.x + xmk.x) * half, (xk.y - xmk.y) * half);
+      C d = mkc((xk.x - xmk.x) * half, (xk.y + xmk.y) * half);
+      C xo = twmul(d, cconj_tw(__ldg(&tw[k])));
+      // Z[k] = xe + i xo ; Z[m-k] = conj(xe - i xo); stored conjugated
+      s[k] = cconj(mkc(xe.x - xo.y, xe.y + xo.x));
+      if (m - k != k) s[m - k] = cconj(mkc(xe.x + xo.y, -(xe.y - xo.x)));
+    }
+    __syncthreads();
+  }
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    Rl *out = (Rl *)a.out.ptr;
+    const Rl sc = (Rl)a.scale;
+    const long long st = a.out.stride;
+    tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
+      C y = line_view<C>(a, l)[j];
+      const long long base = off - (long long)j * st + 2LL * j * st;
+      out[base] = y.x * sc;
+      out[base + st] = -y.y * sc;
+    });
+  }
+};
+
+// Odd (or any) length real forward through a full complex line: reals in the
+// real parts, imaginary parts zero; the first n/2+1 bins are stored.
+struct OpR2CFull {
+  static constexpr bool kConv = false, kFG = true, kTG = true;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int i) {
+    using Rl = typename P::real;
+    if (!c.valid) return mkc((Rl)0, (Rl)0);
+    return mkc(((const Rl *)a.in.ptr)[c.ioff + (long long)i * a.in.stride], (Rl)0);
+  }
+  template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
+    if (!c.valid || i > a.lp.n / 2) return;
+    ((Cx<P> *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = y;
+  }
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    using Rl = typename P::real;
+    const Rl *in = (const Rl *)a.in.ptr;
+    tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
+      Cx<P> *d = &line_view<Cx<P>>(a, l)[i];
+      cp_async_n<sizeof(Rl)>(&d->x, &in[off]);
+      d->y = (Rl)0;
+    });
+  }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    C *out = (C *)a.out.ptr;
+    const int h = a.lp.n / 2 + 1;
+    tile_loop(a.out, a.lpc, h, FastDiv((uint32_t)h), a.lpcdiv, line0, a.nlines,
+              [&](int l, int k, long long off) { out[off] = line_view<C>(a, l)[k]; });
+  }
+};
+
+// Odd (or any) length real inverse through the full Hermitian mirror:
+// element i < n/2+1 is bin i, element i > n/2 is conj(bin(n-i)); bins at or
+// beyond ic read as zero.  Stored conjugated; the real part is the output.
+struct OpC2RFull {
+  static constexpr bool kConv = false, kFG = false, kTG = true;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &, const LineCtx &, int) { return Cx<P>(); }
+  template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
+    using Rl = typename P::real;
+    if (!c.valid) return;
+    ((Rl *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = y.x * (Rl)a.scale;
+  }
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    load_bins<P>(a, line0, a.lp.n / 2 + 1, a.ic & GF_IC_MASK);
+  }
+  template <class P> static GF_DEV void prep(const KArgs &a, long long) {
+    using C = Cx<P>;
+    const int n = a.lp.n;
+    const int h = n / 2 + 1;
+    const int up = n - h;  // mirrored elements i = h .. n-1
+    for (int e = threadIdx.x; e < a.lpc * up; e += blockDim.x) {
+      const int l = e / up, i = h + (e - l * up);
+      const LineView<C> s = line_view<C>(a, l);
+      s[i] = s[n - i];  // conj(conj(bin(n-i)))
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < a.lpc * h; e += blockDim.x) {
+      const int l = e / h, i = e - l * h;
+      const LineView<C> s = line_view<C>(a, l);
+      s[i].y = -s[i].y;
+    }
+    __syncthreads();
+  }
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+    using Rl = typename P::real;
+    Rl *out = (Rl *)a.out.ptr;
+    const Rl sc = (Rl)a.scale;
+    tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
+      out[off] = line_view<Cx<P>>(a, l)[i].x * sc;
+    });
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Rader, fused in one CTA (rader.go:129-172 restated for one line):
+//   a[k] = x[perm[k]] (k < q = p-1, zero-padded to cl), A = FFT_cl(a),
+//   X[0] = x0 + A[0] (= sum of all inputs),
+//   conv = IFFT_cl(A * B)  evaluated as conj(FFT_cl(conj(A * B / cl))),
+//   X[iperm[qi]] = x0 + conv[qi + off]   (off = 0 cyclic, q padded-linear).
+// aux0 = perm (int32, q), aux1 = iperm (int32, q), aux2 = B/cl (sp_t, cl),
+// ia = p, ic = off.  lp is the length-cl program; the extra slots of a line
+// hold x0 and X[0].
+// ---------------------------------------------------------------------------
+struct OpRader {
+  static constexpr bool kConv = true, kFG = true, kTG = true;
+  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int k) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    if (!c.valid) return mkc((Rl)0, (Rl)0);
+    const C *in = (const C *)a.in.ptr;
+    if (k == 0) {
+      C x0 = in[c.ioff];
+      if (a.cj_in) x0.y = -x0.y;
+      line_extra<C>(a, c.l)[0] = x0;
+    }
+    const int q = (int)a.ia - 1;
+    if (k >= q) return mkc((Rl)0, (Rl)0);
+    return in[c.ioff + (long long)__ldg(&((const int *)a.aux0)[k]) * a.in.stride];
+  }
+  template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    const int q = (int)a.ia - 1;
+    const int qi = i - a.ic;
+    if (!c.valid || qi < 0 || qi >= q) return;
+    const C v = cadd(line_extra<C>(a, c.l)[0], cconj(y));
+    const Rl sc = (Rl)a.scale;
+    const long long d = __ldg(&((const int *)a.aux1)[qi]);
+    ((C *)a.out.ptr)[c.ooff + d * a.out.stride] = mkc(v.x * sc, v.y * (a.cj_out ? -sc : sc));
+  }
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    const C *in = (const C *)a.in.ptr;
+    const int *perm = (const int *)a.aux0;
+    const int cl = a.lp.n;
+    const int q = (int)a.ia - 1;
+    const long long st = a.in.stride;
+    tile_loop(a.in, a.lpc, cl, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int k, long long off) {
+      const long long base = off - (long long)k * st;
+      C *d = &line_view<C>(a, l)[k];
+      if (k < q) cp_async_n<sizeof(C)>(d, &in[base + (long long)__ldg(&perm[k]) * st]);
+      else *d = mkc((Rl)0, (Rl)0);
+      if (k == 0) {
+        C x0 = in[base];
+        if (a.cj_in) x0.y = -x0.y;
+        line_extra<C>(a, l)[0] = x0;
+      }
+    });
+  }
+  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
+  template <class P> static GF_DEV void mid(const KArgs &a, long long line0, bool last_g) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    using SP = typename P::sp_t;
+    const SP *B = (const SP *)a.aux2;
+    const int cl = a.lp.n;
+    // X[0] first (reads A[0] before the multiply overwrites it)
+    for (int l = threadIdx.x; l < a.lpc; l += blockDim.x) {
+      C *ex = line_extra<C>(a, l);
+      ex[1] = cadd(ex[0], line_view<C>(a, l)[0]);
+      if (last_g && line0 + l < a.nlines) {
+        const Rl sc = (Rl)a.scale;
+        ((C *)a.out.ptr)[line_off(a.out, (uint32_t)(line0 + l))] =
+            mkc(ex[1].x * sc, ex[1].y * (a.cj_out ? -sc : sc));
+      }
+    }
+    __syncthreads();
+    const int total = a.lpc * cl;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      uint32_t l, k;
+      a.ndiv.divmod((uint32_t)e, l, k);
+      const LineView<C> s = line_view<C>(a, (int)l);
+      s[k] = cconj(spmul(s[k], __ldg(&B[k])));
+    }
+    __syncthreads();
+  }
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    C *out = (C *)a.out.ptr;
+    const int *iperm = (const int *)a.aux1;
+    const int p = (int)a.ia;
+    const int offc = a.ic;
+    const Rl sc = (Rl)a.scale;
+    const Rl sy = a.cj_out ? -sc : sc;
+    const long long st = a.out.stride;
+    tile_loop(a.out, a.lpc, p, FastDiv((uint32_t)p), a.lpcdiv, line0, a.nlines,
+              [&](int l, int i, long long off) {
+                const long long base = off - (long long)i * st;
+                const C *ex = line_extra<C>(a, l);
+                C y;
+                long long dst;
+                if (i == 0) {
+                  y = ex[1];
+                  dst = 0;
+                } else {
+                  y = cadd(ex[0], cconj(line_view<C>(a, l)[i - 1 + offc]));
+                  dst = __ldg(&iperm[i - 1]);
+                }
+                out[base + dst * st] = mkc(y.x * sc, y.y * sy);
+              });
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Bluestein, fused in one CTA (bluestein.go:67-95 restated for one line):
+//   a[j] = x[j] w[j] (j < n, zero-padded to m), conv = IFFT_m(FFT_m(a) * B)
+//   with B = FFT_m(b) / m, evaluated as conj(FFT_m(conj(FFT_m(a) * B))),
+//   X[k] = conv[k] w[k].
+// aux0 = chirp w (sp_t, n), aux2 = B/m (sp_t, m), ia = n.  lp has length m.
+// ---------------------------------------------------------------------------
+struct OpBluestein {
+  static constexpr bool kConv = true, kFG = true, kTG = true;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int j) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    using SP = typename P::sp_t;
+    if (!c.valid || j >= (int)a.ia) return mkc((Rl)0, (Rl)0);
+    C v = ((const C *)a.in.ptr)[c.ioff + (long long)j * a.in.stride];
+    if (a.cj_in) v.y = -v.y;
+    return spmul(v, __ldg(&((const SP *)a.aux0)[j]));
+  }
+  template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int k, Cx<P> y) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    using SP = typename P::sp_t;
+    if (!c.valid || k >= (int)a.ia) return;
+    const C v = spmul(cconj(y), __ldg(&((const SP *)a.aux0)[k]));
+    const Rl sc = (Rl)a.scale;
+    ((C *)a.out.ptr)[c.ooff + (long long)k * a.out.stride] = mkc(v.x * sc, v.y * (a.cj_out ? -sc : sc));
+  }
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    const C *in = (const C *)a.in.ptr;
+    const int n = (int)a.ia;
+    tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
+      C *d = &line_view<C>(a, l)[j];
+      if (j < n) cp_async_n<sizeof(C)>(d, &in[off]);
+      else *d = mkc((Rl)0, (Rl)0);
+    });
+  }
+  // a[j] = conj?(x[j]) * w[j] for j < n
+  template <class P> static GF_DEV void prep(const KArgs &a, long long) {
+    using C = Cx<P>;
+    using SP = typename P::sp_t;
+    const SP *w = (const SP *)a.aux0;
+    const int n = (int)a.ia;
+    for (int e = threadIdx.x; e < a.lpc * n; e += blockDim.x) {
+      const int l = e / n, j = e - l * n;
+      const LineView<C> s = line_view<C>(a, l);
+      C v = s[j];
+      if (a.cj_in) v.y = -v.y;
+      s[j] = spmul(v, __ldg(&w[j]));
+    }
+    __syncthreads();
+  }
+  template <class P> static GF_DEV void mid(const KArgs &a, long long, bool) {
+    using C = Cx<P>;
+    using SP = typename P::sp_t;
+    const SP *B = (const SP *)a.aux2;
+    const int total = a.lpc * a.lp.n;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      uint32_t l, k;
+      a.ndiv.divmod((uint32_t)e, l, k);
+      const LineView<C> s = line_view<C>(a, (int)l);
+      s[k] = cconj(spmul(s[k], __ldg(&B[k])));
+    }
+    __syncthreads();
+  }
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    using SP = typename P::sp_t;
+    C *out = (C *)a.out.ptr;
+    const SP *w = (const SP *)a.aux0;
+    const int n = (int)a.ia;
+    const Rl sc = (Rl)a.scale;
+    const Rl sy = a.cj_out ? -sc : sc;
+    tile_loop(a.out, a.lpc, n, FastDiv((uint32_t)n), a.lpcdiv, line0, a.nlines,
+              [&](int l, int k, long long off) {
+                C y = spmul(cconj(line_view<C>(a, l)[k]), __ldg(&w[k]));
+                out[off] = mkc(y.x * sc, y.y * sy);
+              });
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Spectrogram frame (freq.go:107-127 with PSD freq.go:69-90): line t is the
+// frame x[t*step .. t*step+seg) times the window, transformed as an even
+// real line (seg = 2m) and reduced to the one-sided density
+//   p[k] = |X[k]|^2 * scale, doubled except for k = 0 and k = m.
+// in: real signal (Side: dist_b = step per frame, stride 1); aux1 = window
+// (real, seg); aux0 = W_2m^k table; out: real bins (m+1 per frame).
+// ---------------------------------------------------------------------------
+struct OpSpectro {
+  static constexpr bool kConv = false, kFG = true, kTG = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int j) {
+    using Rl = typename P::real;
+    if (!c.valid) return mkc((Rl)0, (Rl)0);
+    const Rl *win = (const Rl *)a.aux1;
+    const Cx<P> v = read_pair<P>(a, c.ioff + 2LL * j, 1);
+    return mkc(v.x * __ldg(&win[2 * j]), v.y * __ldg(&win[2 * j + 1]));
+  }
+  template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+    tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
+      // stride 1: complex element j sits at off = line + j; its real pair is
+      // at line + 2j = off + j
+      load_real_pair<P>(a, &line_view<Cx<P>>(a, l)[j], off + j, 1);
+    });
+  }
+  template <class P> static GF_DEV void prep(const KArgs &a, long long) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    const Rl *win = (const Rl *)a.aux1;
+    const int m = a.lp.n;
+    for (int e = threadIdx.x; e < a.lpc * m; e += blockDim.x) {
+      const int l = e / m, j = e - l * m;
+      const LineView<C> s = line_view<C>(a, l);
+      C v = s[j];
+      s[j] = mkc(v.x * __ldg(&win[2 * j]), v.y * __ldg(&win[2 * j + 1]));
+    }
+    __syncthreads();
+  }
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+    using Rl = typename P::real;
+    Rl *out = (Rl *)a.out.ptr;
+    const Rl sc = (Rl)a.scale;
+    const int m = a.lp.n;
+    untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) {
+      Rl pw = (v.x * v.x + v.y * v.y) * sc;
+      if (k != 0 && k != m) pw *= (Rl)2;
+      out[base + k] = pw;
+    });
+  }
+};
+
+}  // namespace gf

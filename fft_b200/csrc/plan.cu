@@ -403,6 +403,34 @@ bool pairs_aligned(const Side &s, int prec) {
          (s.lpb.d == 1 || (s.dist_l % 2) == 0);
 }
 
+// Whether an op can read its first stage / write its last stage directly.
+static bool op_fg(int op) {
+  return op == OP_C2C || op == OP_C2C_TW || op == OP_R2C || op == OP_R2C_FULL || op == OP_RADER ||
+         op == OP_BLUE || op == OP_SPECTRO;
+}
+static bool op_tg(int op) {
+  return op == OP_C2C || op == OP_C2C_TW || op == OP_C2R || op == OP_R2C_FULL || op == OP_C2R_FULL ||
+         op == OP_RADER || op == OP_BLUE;
+}
+// A side is column-like when adjacent lines sit closer than adjacent elements
+// (a non-contiguous axis of a row-major array): threads then map across lines.
+static bool side_col(const Side &s) {
+  if (s.stride == 1) return false;
+  const long long D = s.lpb.d > 1 ? s.dist_l : s.dist_b;
+  return std::llabs(D) < std::llabs(s.stride);
+}
+static int choose_flags(int op, const KArgs &a) {
+  const bool fg = op_fg(op), tg = op_tg(op);
+  const bool ic = side_col(a.in), oc = side_col(a.out);
+  if (fg && tg) {
+    if (ic == oc) return (ic ? GF_COLMAP : 0) | GF_FIRST_DIRECT | GF_LAST_DIRECT;
+    return (ic ? GF_COLMAP : 0) | GF_FIRST_DIRECT;
+  }
+  if (fg) return (ic ? GF_COLMAP : 0) | GF_FIRST_DIRECT;
+  if (tg) return (oc ? GF_COLMAP : 0) | GF_LAST_DIRECT;
+  return 0;
+}
+
 int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st, int lpc,
                 bool conv) {
   if (nlines <= 0) return 0;
@@ -413,6 +441,10 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   a.lpc = lpc;
   a.ndiv = FastDiv((uint32_t)dp.n);
   a.lpcdiv = FastDiv((uint32_t)lpc);
+  a.flags = choose_flags(op, a);
+  if (const char *e = getenv("GOFFT_NO_DIRECT")) {
+    if (*e == '1') a.flags &= GF_COLMAP;
+  }
   const size_t smem = (size_t)lpc * spad_size(dp.n) * csize(dp.prec) + (conv ? 2 * lpc * csize(dp.prec) : 0);
   KFn f = kernel_for(dp.prec, dp.maxe, op);
   if (!f) return set_err(5, "no kernel instance for this precision/op");
@@ -431,7 +463,8 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   if (timed) {
     cudaEventRecord(rec.b, st);
     std::ostringstream k;
-    k << op_name(op) << "/n=" << dp.n << "/prec=" << dp.prec << "/lpc=" << lpc << "/T=" << dp.lp.T;
+    k << op_name(op) << "/n=" << dp.n << "/prec=" << dp.prec << "/lpc=" << lpc << "/T=" << dp.lp.T
+      << "/flags=" << a.flags;
     rec.key = k.str();
     rec.bytes = algo_bytes(op, dp, a, nlines);
     std::lock_guard<std::mutex> lk(g_tmu);
@@ -852,7 +885,7 @@ int ExecReal::c2r(const Side &in, int nb, const Side &out, long long nl, double 
       a.in = in;
       a.out = out;
       a.aux0 = tw2;
-      a.ic = nb;
+      a.ic = nb | (pairs_aligned(out, prec) ? GF_PAIR_ALIGNED : 0);
       a.scale = scale / (double)m;
       return launch_line(OP_C2R, *cx->prog, a, nl, st);
     }
