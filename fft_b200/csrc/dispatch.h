@@ -25,6 +25,11 @@ typedef void (*KFn)(KArgs);
 KFn line_kernel_f64(int maxe, int op);
 KFn line_kernel_f32(int maxe, int op);
 KFn line_kernel_f32c(int maxe, int op);
+// Compile-time-schedule instance for (n, threads per line, lines per CTA, op,
+// schedule), or nullptr.
+KFn line_kernel_ct_f64(int n, int T, int lpc, int op, const int *rad, int nst);
+KFn line_kernel_ct_f32(int n, int T, int lpc, int op, const int *rad, int nst);
+KFn line_kernel_ct_f32c(int n, int T, int lpc, int op, const int *rad, int nst);
 
 // Elementwise / table kernels of one precision, launched on `st`.
 struct EwArgs {

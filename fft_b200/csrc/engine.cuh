@@ -299,4 +299,107 @@ GF_DEV void tile_loop(const Side &sd, int lpc, int len, FastDiv ldiv, FastDiv lp
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Compile-time schedules.  For the hot lengths the radix list, the threads
+// per line and the lines per CTA are template parameters: every stage is
+// straight-line code with constant strides, so divisions become shifts, the
+// butterfly guards vanish, and the kernel body is only as long as its own
+// stages (the run-time schedule kernel carries every radix and thrashes the
+// instruction cache).  The twiddle table layout is the run-time one.
+// ---------------------------------------------------------------------------
+template <int... Rs> struct Sched {};
+
+template <int N, int T, int R> constexpr int ct_per() { return ((N / R) + T - 1) / T; }
+template <int N, int T> constexpr int ct_maxe() { return 0; }
+template <int N, int T, int R, int... Rs> constexpr int ct_maxe_r() {
+  constexpr int here = ct_per<N, T, R>() * R;
+  if constexpr (sizeof...(Rs) == 0) return here;
+  else {
+    constexpr int rest = ct_maxe_r<N, T, Rs...>();
+    return here > rest ? here : rest;
+  }
+}
+
+template <class P, class Op, int N, int T, int NS, int R, int E, bool FG, bool TG>
+GF_DEV void stage_ct(typename P::cpx (&v)[E], const LineView<typename P::cpx> &s, const KArgs &a,
+                     const LineCtx &c, const typename P::tw_t *tw, bool cj) {
+  using C = typename P::cpx;
+  constexpr int NB = N / R;
+  constexpr int PER = (NB + T - 1) / T;
+  constexpr bool EXACT = (NB % T) == 0;
+#pragma unroll
+  for (int b = 0; b < PER; b++) {
+    const int j = c.t + b * T;
+    if (EXACT || j < NB) {
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        C x;
+        if constexpr (FG) x = Op::template gload<P>(a, c, j + r * NB);
+        else x = s[j + r * NB];
+        if (cj) x.y = -x.y;
+        v[b * R + r] = x;
+      }
+    }
+  }
+  if constexpr (!FG) __syncthreads();
+#pragma unroll
+  for (int b = 0; b < PER; b++) {
+    const int j = c.t + b * T;
+    if (EXACT || j < NB) {
+      const int q = j / NS, k = j % NS;
+      if constexpr (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; r++)
+          v[b * R + r] = twmul(v[b * R + r], __ldg(&tw[(r - 1) * NS + k]));
+      }
+      Dft<R, C>::run(&v[b * R]);
+      const int base = q * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        if constexpr (TG) Op::template gstore<P>(a, c, base + r * NS, v[b * R + r]);
+        else s[base + r * NS] = v[b * R + r];
+      }
+    }
+  }
+  if constexpr (!TG) __syncthreads();
+}
+
+template <class P, class Op, int N, int T, int NS, int TO, int E, bool CAN_FG, bool CAN_TG, int R,
+          int... Rs>
+GF_DEV void stages_ct(typename P::cpx (&v)[E], const LineView<typename P::cpx> &s, const KArgs &a,
+                      const LineCtx &c, bool cj_first, bool fg, bool tg) {
+  using TW = typename P::tw_t;
+  constexpr bool FIRST = NS == 1;
+  constexpr bool LAST = sizeof...(Rs) == 0;
+  const TW *tw = (const TW *)a.lp.tw + TO;
+  const bool cj = FIRST && cj_first;
+  constexpr bool F_OK = FIRST && CAN_FG;
+  constexpr bool T_OK = LAST && CAN_TG;
+  if constexpr (F_OK && T_OK) {
+    if (fg && tg) stage_ct<P, Op, N, T, NS, R, E, true, true>(v, s, a, c, tw, cj);
+    else if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false>(v, s, a, c, tw, cj);
+    else if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true>(v, s, a, c, tw, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false>(v, s, a, c, tw, cj);
+  } else if constexpr (F_OK) {
+    if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false>(v, s, a, c, tw, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false>(v, s, a, c, tw, cj);
+  } else if constexpr (T_OK) {
+    if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true>(v, s, a, c, tw, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false>(v, s, a, c, tw, cj);
+  } else {
+    stage_ct<P, Op, N, T, NS, R, E, false, false>(v, s, a, c, tw, cj);
+  }
+  if constexpr (!LAST)
+    stages_ct<P, Op, N, T, NS * R, TO + NS * (R - 1), E, CAN_FG, CAN_TG, Rs...>(v, s, a, c, cj_first, fg, tg);
+}
+
+template <class P, class Op, int N, int T, bool CAN_FG, bool CAN_TG, int... Rs>
+GF_DEV void run_stages_ct(Sched<Rs...>, const LineView<typename P::cpx> &s, const KArgs &a,
+                          const LineCtx &c, bool cj_first, bool fg, bool tg) {
+  constexpr int E = ct_maxe_r<N, T, Rs...>();
+  typename P::cpx v[E];
+  stages_ct<P, Op, N, T, 1, 0, E, CAN_FG, CAN_TG, Rs...>(v, s, a, c, cj_first, fg, tg);
+}
+
 }  // namespace gf

@@ -31,6 +31,60 @@ template <class P> KFn pick_maxe(int maxe, int op) {
   return nullptr;
 }
 
+// Compile-time schedules: (N, threads per line, lines per CTA, row-ops too,
+// radices...).  Each length has the run-time heuristic's lines per CTA and
+// twice that (column transforms of FP32 data); the schedules are those
+// gpu_radices() and pick_threads() derive for the length.
+#define GF_CT_LIST(X)                                                     \
+  X(64, 4, 64, 1, 8, 8) X(64, 4, 128, 0, 8, 8)                           \
+  X(128, 8, 32, 1, 16, 8) X(128, 8, 64, 0, 16, 8)                        \
+  X(256, 16, 16, 1, 16, 16) X(256, 16, 32, 0, 16, 16)                    \
+  X(512, 32, 8, 1, 8, 8, 8) X(512, 32, 16, 0, 8, 8, 8)                   \
+  X(1024, 64, 4, 1, 16, 8, 8) X(1024, 64, 8, 0, 16, 8, 8)                \
+  X(2048, 128, 2, 1, 16, 16, 8) X(2048, 128, 4, 0, 16, 16, 8)            \
+  X(4096, 256, 1, 1, 16, 16, 16) X(4096, 256, 2, 0, 16, 16, 16)          \
+  X(8192, 512, 1, 1, 16, 8, 8, 8)                                         \
+  X(16384, 512, 1, 1, 16, 16, 8, 8)
+
+template <int... Rs> constexpr bool sched_eq(const int *r, int nst) {
+  constexpr int a[] = {Rs...};
+  if (nst != (int)sizeof...(Rs)) return false;
+  for (int i = 0; i < nst; i++)
+    if (a[i] != r[i]) return false;
+  return true;
+}
+
+template <class P, int N, int T, int L, bool ROWOPS, int... Rs> KFn ct_for(int op) {
+  using S = Sched<Rs...>;
+  constexpr int MINB = (L * T <= 256) ? 2 : 1;
+  if constexpr (N == 16384) {
+    if constexpr (sizeof(typename P::cpx) == 16) return nullptr;  // FP64 16384 is two-pass
+  }
+  switch (op) {
+    case OP_C2C: return k_line_ct<P, N, T, L, MINB, OpC2C, S>;
+    case OP_C2C_TW: return k_line_ct<P, N, T, L, MINB, OpC2CTwiddle, S>;
+    default: break;
+  }
+  if constexpr (ROWOPS) {
+    switch (op) {
+      case OP_R2C: return k_line_ct<P, N, T, L, MINB, OpR2CPacked, S>;
+      case OP_C2R: return k_line_ct<P, N, T, L, MINB, OpC2RPacked, S>;
+      case OP_SPECTRO: return k_line_ct<P, N, T, L, MINB, OpSpectro, S>;
+      default: break;
+    }
+  }
+  return nullptr;
+}
+
+template <class P> KFn pick_ct(int n, int T, int lpc, int op, const int *rad, int nst) {
+#define GF_CT_X(N, TT, L, ROW, ...)                                           \
+  if (n == N && T == TT && lpc == L && sched_eq<__VA_ARGS__>(rad, nst))      \
+    return ct_for<P, N, TT, L, ROW != 0, __VA_ARGS__>(op);
+  GF_CT_LIST(GF_CT_X)
+#undef GF_CT_X
+  return nullptr;
+}
+
 static inline int ew_blocks(long long total) {
   long long b = (total + 255) / 256;
   if (b > 148 * 32) b = 148 * 32;
@@ -44,6 +98,9 @@ static inline int ew_blocks(long long total) {
   namespace gf {                                                                               \
   KFn line_kernel_##SUFFIX(int maxe, int op) {                                                 \
     return pick_maxe<P>(maxe, op);                                                             \
+  }                                                                                            \
+  KFn line_kernel_ct_##SUFFIX(int n, int T, int lpc, int op, const int *rad, int nst) {        \
+    return pick_ct<P>(n, T, lpc, op, rad, nst);                                                \
   }                                                                                            \
   namespace prec_##SUFFIX {                                                                    \
   using C = P::cpx;                                                                            \

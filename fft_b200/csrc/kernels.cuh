@@ -47,6 +47,41 @@ __global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
   if (!last_g) Op::template store<P>(a, line0);
 }
 
+
+// ---------------------------------------------------------------------------
+// Compile-time-schedule line kernel (hot power-of-two lengths): same phases as
+// k_line, with N, T, the lines per CTA and the radix list fixed.  Not used for
+// the convolution ops.
+// ---------------------------------------------------------------------------
+template <class P, int N, int T, int LPC, int MINB, class Op, class S>
+__global__ void __launch_bounds__(LPC *T, MINB) k_line_ct(const KArgs a) {
+  using C = typename P::cpx;
+  const long long line0 = (long long)blockIdx.x * LPC;
+  LineCtx c;
+  if (a.flags & GF_COLMAP) {
+    c.l = threadIdx.x % LPC;
+    c.t = threadIdx.x / LPC;
+  } else {
+    c.l = threadIdx.x / T;
+    c.t = threadIdx.x % T;
+  }
+  c.line = line0 + c.l;
+  c.valid = c.line < a.nlines;
+  c.ioff = c.valid ? line_off(a.in, (uint32_t)c.line) : 0;
+  c.ooff = c.valid ? line_off(a.out, (uint32_t)c.line) : 0;
+  const bool first_g = Op::kFG && (a.flags & GF_FIRST_DIRECT);
+  const bool last_g = Op::kTG && (a.flags & GF_LAST_DIRECT);
+  if (!first_g) {
+    Op::template load<P>(a, line0);
+    cp_async_wait_all();
+    __syncthreads();
+    Op::template prep<P>(a, line0);
+  }
+  const LineView<C> s = line_view<C>(a, c.l);
+  run_stages_ct<P, Op, N, T, Op::kFG, Op::kTG>(S{}, s, a, c, Op::first_conj(a), first_g, last_g);
+  if (!last_g) Op::template store<P>(a, line0);
+}
+
 // ===========================================================================
 // Table generation (FP64 on the device; exact integer angle reduction).
 // ===========================================================================

@@ -154,6 +154,14 @@ static KFn kernel_for(int prec, int maxe, int op) {
   }
 }
 
+static KFn kernel_ct_for(const DevProg &dp, int op, int lpc) {
+  switch (dp.prec) {
+    case F64: return line_kernel_ct_f64(dp.n, dp.lp.T, lpc, op, dp.lp.radix, dp.lp.nst);
+    case F32: return line_kernel_ct_f32(dp.n, dp.lp.T, lpc, op, dp.lp.radix, dp.lp.nst);
+    default: return line_kernel_ct_f32c(dp.n, dp.lp.T, lpc, op, dp.lp.radix, dp.lp.nst);
+  }
+}
+
 static int ensure_smem(KFn f, size_t smem) {
   static std::mutex mu;
   static std::map<std::pair<int, const void *>, size_t> done;
@@ -446,7 +454,10 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
     if (*e == '1') a.flags &= GF_COLMAP;
   }
   const size_t smem = (size_t)lpc * spad_size(dp.n) * csize(dp.prec) + (conv ? 2 * lpc * csize(dp.prec) : 0);
-  KFn f = kernel_for(dp.prec, dp.maxe, op);
+  KFn f = nullptr;
+  static const bool no_ct = getenv("GOFFT_NO_CT") && getenv("GOFFT_NO_CT")[0] == '1';
+  if (!conv && !no_ct) f = kernel_ct_for(dp, op, lpc);
+  if (!f) f = kernel_for(dp.prec, dp.maxe, op);
   if (!f) return set_err(5, "no kernel instance for this precision/op");
   if (int rc = ensure_smem(f, smem)) return rc;
   const long long grid = (nlines + lpc - 1) / lpc;
