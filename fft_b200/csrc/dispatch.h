@@ -21,15 +21,23 @@ enum Op {
 
 typedef void (*KFn)(KArgs);
 
-// Line kernel for (maxe, op) in each precision; nullptr if not instantiated.
-KFn line_kernel_f64(int maxe, int op);
-KFn line_kernel_f32(int maxe, int op);
-KFn line_kernel_f32c(int maxe, int op);
+// Run-time-schedule line kernel for (maxe, op) in each precision and op group
+// (0: complex and convolution ops, 1: real ops); nullptr if not instantiated.
+KFn line_kernel_f64_0(int maxe, int op);
+KFn line_kernel_f64_1(int maxe, int op);
+KFn line_kernel_f32_0(int maxe, int op);
+KFn line_kernel_f32_1(int maxe, int op);
+KFn line_kernel_f32c_0(int maxe, int op);
+KFn line_kernel_f32c_1(int maxe, int op);
 // Compile-time-schedule instance for (n, threads per line, lines per CTA, op,
 // schedule), or nullptr.
-KFn line_kernel_ct_f64(int n, int T, int lpc, int op, const int *rad, int nst);
-KFn line_kernel_ct_f32(int n, int T, int lpc, int op, const int *rad, int nst);
-KFn line_kernel_ct_f32c(int n, int T, int lpc, int op, const int *rad, int nst);
+// (group 0: C2C and four-step twiddle; group 1: real-row ops)
+KFn line_kernel_ct_f64_0(int n, int T, int lpc, int op, const int *rad, int nst);
+KFn line_kernel_ct_f64_1(int n, int T, int lpc, int op, const int *rad, int nst);
+KFn line_kernel_ct_f32_0(int n, int T, int lpc, int op, const int *rad, int nst);
+KFn line_kernel_ct_f32_1(int n, int T, int lpc, int op, const int *rad, int nst);
+KFn line_kernel_ct_f32c_0(int n, int T, int lpc, int op, const int *rad, int nst);
+KFn line_kernel_ct_f32c_1(int n, int T, int lpc, int op, const int *rad, int nst);
 
 // Elementwise / table kernels of one precision, launched on `st`.
 struct EwArgs {

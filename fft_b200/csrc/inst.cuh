@@ -6,27 +6,34 @@
 
 namespace gf {
 
-template <class P, int M> KFn pick_line(int op) {
-  switch (op) {
-    case OP_C2C: return k_line<P, M, OpC2C>;
-    case OP_C2C_TW: return k_line<P, M, OpC2CTwiddle>;
-    case OP_R2C: return k_line<P, M, OpR2CPacked>;
-    case OP_C2R: return k_line<P, M, OpC2RPacked>;
-    case OP_R2C_FULL: return k_line<P, M, OpR2CFull>;
-    case OP_C2R_FULL: return k_line<P, M, OpC2RFull>;
-    case OP_RADER: return k_line<P, M, OpRader>;
-    case OP_BLUE: return k_line<P, M, OpBluestein>;
-    case OP_SPECTRO: return k_line<P, M, OpSpectro>;
-    default: return nullptr;
+// GROUP 0: complex and convolution ops; GROUP 1: real ops.
+template <class P, int M, int GROUP> KFn pick_line(int op) {
+  if constexpr (GROUP == 0) {
+    switch (op) {
+      case OP_C2C: return k_line<P, M, OpC2C>;
+      case OP_C2C_TW: return k_line<P, M, OpC2CTwiddle>;
+      case OP_RADER: return k_line<P, M, OpRader>;
+      case OP_BLUE: return k_line<P, M, OpBluestein>;
+      default: return nullptr;
+    }
+  } else {
+    switch (op) {
+      case OP_R2C: return k_line<P, M, OpR2CPacked>;
+      case OP_C2R: return k_line<P, M, OpC2RPacked>;
+      case OP_R2C_FULL: return k_line<P, M, OpR2CFull>;
+      case OP_C2R_FULL: return k_line<P, M, OpC2RFull>;
+      case OP_SPECTRO: return k_line<P, M, OpSpectro>;
+      default: return nullptr;
+    }
   }
 }
 
 // FP64 lines use 16 register elements per thread (32 would spill); the FP32
 // forms also get a 32-element variant for lines longer than 16 x 512.
-template <class P> KFn pick_maxe(int maxe, int op) {
-  if (maxe == 16) return pick_line<P, 16>(op);
+template <class P, int GROUP> KFn pick_maxe(int maxe, int op) {
+  if (maxe == 16) return pick_line<P, 16, GROUP>(op);
   if constexpr (sizeof(typename P::cpx) == 8) {
-    if (maxe == 32) return pick_line<P, 32>(op);
+    if (maxe == 32) return pick_line<P, 32, GROUP>(op);
   }
   return nullptr;
 }
@@ -54,32 +61,34 @@ template <int... Rs> constexpr bool sched_eq(const int *r, int nst) {
   return true;
 }
 
-template <class P, int N, int T, int L, bool ROWOPS, int... Rs> KFn ct_for(int op) {
+// GROUP 0: complex ops (C2C, four-step twiddle); GROUP 1: real-row ops.
+template <class P, int GROUP, int N, int T, int L, bool ROWOPS, int... Rs> KFn ct_for(int op) {
   using S = Sched<Rs...>;
   constexpr int MINB = (L * T <= 256) ? 2 : 1;
-  if constexpr (N == 16384) {
-    if constexpr (sizeof(typename P::cpx) == 16) return nullptr;  // FP64 16384 is two-pass
-  }
-  switch (op) {
-    case OP_C2C: return k_line_ct<P, N, T, L, MINB, OpC2C, S>;
-    case OP_C2C_TW: return k_line_ct<P, N, T, L, MINB, OpC2CTwiddle, S>;
-    default: break;
-  }
-  if constexpr (ROWOPS) {
+  if constexpr (N == 16384 && sizeof(typename P::cpx) == 16) {
+    return nullptr;  // FP64 16384 is two-pass
+  } else if constexpr (GROUP == 0) {
+    switch (op) {
+      case OP_C2C: return k_line_ct<P, N, T, L, MINB, OpC2C, S>;
+      case OP_C2C_TW: return k_line_ct<P, N, T, L, MINB, OpC2CTwiddle, S>;
+      default: return nullptr;
+    }
+  } else if constexpr (ROWOPS) {
     switch (op) {
       case OP_R2C: return k_line_ct<P, N, T, L, MINB, OpR2CPacked, S>;
       case OP_C2R: return k_line_ct<P, N, T, L, MINB, OpC2RPacked, S>;
       case OP_SPECTRO: return k_line_ct<P, N, T, L, MINB, OpSpectro, S>;
-      default: break;
+      default: return nullptr;
     }
+  } else {
+    return nullptr;
   }
-  return nullptr;
 }
 
-template <class P> KFn pick_ct(int n, int T, int lpc, int op, const int *rad, int nst) {
+template <class P, int GROUP> KFn pick_ct(int n, int T, int lpc, int op, const int *rad, int nst) {
 #define GF_CT_X(N, TT, L, ROW, ...)                                           \
   if (n == N && T == TT && lpc == L && sched_eq<__VA_ARGS__>(rad, nst))      \
-    return ct_for<P, N, TT, L, ROW != 0, __VA_ARGS__>(op);
+    return ct_for<P, GROUP, N, TT, L, ROW != 0, __VA_ARGS__>(op);
   GF_CT_LIST(GF_CT_X)
 #undef GF_CT_X
   return nullptr;
@@ -96,12 +105,6 @@ static inline int ew_blocks(long long total) {
 
 #define GF_DEFINE_PREC(P, SUFFIX)                                                              \
   namespace gf {                                                                               \
-  KFn line_kernel_##SUFFIX(int maxe, int op) {                                                 \
-    return pick_maxe<P>(maxe, op);                                                             \
-  }                                                                                            \
-  KFn line_kernel_ct_##SUFFIX(int n, int T, int lpc, int op, const int *rad, int nst) {        \
-    return pick_ct<P>(n, T, lpc, op, rad, nst);                                                \
-  }                                                                                            \
   namespace prec_##SUFFIX {                                                                    \
   using C = P::cpx;                                                                            \
   using SP = P::sp_t;                                                                          \
@@ -177,4 +180,19 @@ static inline int ew_blocks(long long total) {
     return cudaGetLastError();                                                                 \
   }                                                                                            \
   }                                                                                            \
+  }
+
+// Compile-time-schedule instances of one precision and op group (their own
+// translation units, so the build parallelises).
+#define GF_DEFINE_CT(P, SUFFIX, GROUP)                                                         \
+  namespace gf {                                                                               \
+  KFn line_kernel_ct_##SUFFIX##_##GROUP(int n, int T, int lpc, int op, const int *rad, int nst) { \
+    return pick_ct<P, GROUP>(n, T, lpc, op, rad, nst);                                         \
+  }                                                                                            \
+  }
+
+// Run-time-schedule instances of one precision and op group.
+#define GF_DEFINE_GEN(P, SUFFIX, GROUP)                                                        \
+  namespace gf {                                                                               \
+  KFn line_kernel_##SUFFIX##_##GROUP(int maxe, int op) { return pick_maxe<P, GROUP>(maxe, op); } \
   }

@@ -14,6 +14,8 @@ namespace gf {
 // ---------------------------------------------------------------------------
 template <class P, int MAXE, class Op>
 __global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
+  // The run-time-schedule kernel always uses the tile prologue / epilogue:
+  // direct stages would multiply its (already long) body by four.
   using C = typename P::cpx;
   const long long line0 = (long long)blockIdx.x * a.lpc;
   LineCtx c;
@@ -26,27 +28,22 @@ __global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
   }
   c.line = line0 + c.l;
   c.valid = c.line < a.nlines;
-  c.ioff = c.valid ? line_off(a.in, (uint32_t)c.line) : 0;
-  c.ooff = c.valid ? line_off(a.out, (uint32_t)c.line) : 0;
-  const bool first_g = Op::kFG && (a.flags & GF_FIRST_DIRECT);
-  const bool last_g = Op::kTG && (a.flags & GF_LAST_DIRECT);
-  if (!first_g) {
-    Op::template load<P>(a, line0);
-    cp_async_wait_all();
-    __syncthreads();
-    Op::template prep<P>(a, line0);
-  }
+  c.ioff = 0;
+  c.ooff = 0;
+  Op::template load<P>(a, line0);
+  cp_async_wait_all();
+  __syncthreads();
+  Op::template prep<P>(a, line0);
   const LineView<C> s = line_view<C>(a, c.l);
   if constexpr (Op::kConv) {
-    run_stages<P, Op, MAXE, Op::kFG, false>(s, a, c, Op::first_conj(a), first_g, false);
-    Op::template mid<P>(a, line0, last_g);
-    run_stages<P, Op, MAXE, false, Op::kTG>(s, a, c, false, false, last_g);
+    run_stages<P, Op, MAXE, false, false>(s, a, c, Op::first_conj(a), false, false);
+    Op::template mid<P>(a, line0, false);
+    run_stages<P, Op, MAXE, false, false>(s, a, c, false, false, false);
   } else {
-    run_stages<P, Op, MAXE, Op::kFG, Op::kTG>(s, a, c, Op::first_conj(a), first_g, last_g);
+    run_stages<P, Op, MAXE, false, false>(s, a, c, Op::first_conj(a), false, false);
   }
-  if (!last_g) Op::template store<P>(a, line0);
+  Op::template store<P>(a, line0);
 }
-
 
 // ---------------------------------------------------------------------------
 // Compile-time-schedule line kernel (hot power-of-two lengths): same phases as

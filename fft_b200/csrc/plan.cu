@@ -147,18 +147,22 @@ static size_t max_smem_optin() {
 }
 
 static KFn kernel_for(int prec, int maxe, int op) {
+  const bool g0 = op == OP_C2C || op == OP_C2C_TW || op == OP_RADER || op == OP_BLUE;
   switch (prec) {
-    case F64: return line_kernel_f64(maxe, op);
-    case F32: return line_kernel_f32(maxe, op);
-    default: return line_kernel_f32c(maxe, op);
+    case F64: return g0 ? line_kernel_f64_0(maxe, op) : line_kernel_f64_1(maxe, op);
+    case F32: return g0 ? line_kernel_f32_0(maxe, op) : line_kernel_f32_1(maxe, op);
+    default: return g0 ? line_kernel_f32c_0(maxe, op) : line_kernel_f32c_1(maxe, op);
   }
 }
 
 static KFn kernel_ct_for(const DevProg &dp, int op, int lpc) {
+  const bool g0 = op == OP_C2C || op == OP_C2C_TW;
+  const int n = dp.n, T = dp.lp.T, nst = dp.lp.nst;
+  const int *r = dp.lp.radix;
   switch (dp.prec) {
-    case F64: return line_kernel_ct_f64(dp.n, dp.lp.T, lpc, op, dp.lp.radix, dp.lp.nst);
-    case F32: return line_kernel_ct_f32(dp.n, dp.lp.T, lpc, op, dp.lp.radix, dp.lp.nst);
-    default: return line_kernel_ct_f32c(dp.n, dp.lp.T, lpc, op, dp.lp.radix, dp.lp.nst);
+    case F64: return g0 ? line_kernel_ct_f64_0(n, T, lpc, op, r, nst) : line_kernel_ct_f64_1(n, T, lpc, op, r, nst);
+    case F32: return g0 ? line_kernel_ct_f32_0(n, T, lpc, op, r, nst) : line_kernel_ct_f32_1(n, T, lpc, op, r, nst);
+    default: return g0 ? line_kernel_ct_f32c_0(n, T, lpc, op, r, nst) : line_kernel_ct_f32c_1(n, T, lpc, op, r, nst);
   }
 }
 
@@ -457,7 +461,11 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   KFn f = nullptr;
   static const bool no_ct = getenv("GOFFT_NO_CT") && getenv("GOFFT_NO_CT")[0] == '1';
   if (!conv && !no_ct) f = kernel_ct_for(dp, op, lpc);
-  if (!f) f = kernel_for(dp.prec, dp.maxe, op);
+  if (!f) {
+    // the run-time-schedule kernel has no direct stages
+    f = kernel_for(dp.prec, dp.maxe, op);
+    a.flags &= GF_COLMAP;
+  }
   if (!f) return set_err(5, "no kernel instance for this precision/op");
   if (int rc = ensure_smem(f, smem)) return rc;
   const long long grid = (nlines + lpc - 1) / lpc;
