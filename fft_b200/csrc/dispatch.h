@@ -31,13 +31,14 @@ KFn line_kernel_f32c_0(int maxe, int op);
 KFn line_kernel_f32c_1(int maxe, int op);
 // Compile-time-schedule instance for (n, threads per line, lines per CTA, op,
 // schedule), or nullptr.
-// (group 0: C2C and four-step twiddle; group 1: real-row ops)
-KFn line_kernel_ct_f64_0(int n, int T, int lpc, int op, const int *rad, int nst);
-KFn line_kernel_ct_f64_1(int n, int T, int lpc, int op, const int *rad, int nst);
-KFn line_kernel_ct_f32_0(int n, int T, int lpc, int op, const int *rad, int nst);
-KFn line_kernel_ct_f32_1(int n, int T, int lpc, int op, const int *rad, int nst);
-KFn line_kernel_ct_f32c_0(int n, int T, int lpc, int op, const int *rad, int nst);
-KFn line_kernel_ct_f32c_1(int n, int T, int lpc, int op, const int *rad, int nst);
+// (group 0: C2C and four-step twiddle; group 1: real-row ops; pipe: the
+// persistent double-buffered variant)
+KFn line_kernel_ct_f64_0(int n, int T, int lpc, int op, const int *rad, int nst, bool pipe);
+KFn line_kernel_ct_f64_1(int n, int T, int lpc, int op, const int *rad, int nst, bool pipe);
+KFn line_kernel_ct_f32_0(int n, int T, int lpc, int op, const int *rad, int nst, bool pipe);
+KFn line_kernel_ct_f32_1(int n, int T, int lpc, int op, const int *rad, int nst, bool pipe);
+KFn line_kernel_ct_f32c_0(int n, int T, int lpc, int op, const int *rad, int nst, bool pipe);
+KFn line_kernel_ct_f32c_1(int n, int T, int lpc, int op, const int *rad, int nst, bool pipe);
 
 // Elementwise / table kernels of one precision, launched on `st`.
 struct EwArgs {

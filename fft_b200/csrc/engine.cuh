@@ -102,8 +102,10 @@ template <class C> struct LineView {
   GF_DEV C &operator[](int i) const { return b[spad(i) * step]; }
 };
 
-template <class C> GF_DEV LineView<C> line_view(const KArgs &a, int l) {
-  C *s = smem_base<C>();
+// View of local line l in the tile buffer starting at sbase (the dynamic
+// shared memory by default; persistent kernels alternate two buffers).
+template <class C> GF_DEV LineView<C> line_view(const KArgs &a, int l, void *sbase = nullptr) {
+  C *s = sbase ? reinterpret_cast<C *>(sbase) : smem_base<C>();
   LineView<C> v;
   if (a.flags & GF_COLMAP) {
     v.b = s + l;

@@ -62,22 +62,26 @@ template <int... Rs> constexpr bool sched_eq(const int *r, int nst) {
 }
 
 // GROUP 0: complex ops (C2C, four-step twiddle); GROUP 1: real-row ops.
-template <class P, int GROUP, int N, int T, int L, bool ROWOPS, int... Rs> KFn ct_for(int op) {
+// PIPE selects the persistent double-buffered kernel.
+template <class P, int GROUP, int N, int T, int L, bool ROWOPS, int... Rs> KFn ct_for(int op, bool pipe) {
   using S = Sched<Rs...>;
   constexpr int MINB = (L * T <= 256) ? 2 : 1;
   if constexpr (N == 16384 && sizeof(typename P::cpx) == 16) {
     return nullptr;  // FP64 16384 is two-pass
   } else if constexpr (GROUP == 0) {
     switch (op) {
-      case OP_C2C: return k_line_ct<P, N, T, L, MINB, OpC2C, S>;
-      case OP_C2C_TW: return k_line_ct<P, N, T, L, MINB, OpC2CTwiddle, S>;
+      case OP_C2C: return pipe ? k_line_pp<P, N, T, L, MINB, OpC2C, S> : k_line_ct<P, N, T, L, MINB, OpC2C, S>;
+      case OP_C2C_TW:
+        return pipe ? k_line_pp<P, N, T, L, MINB, OpC2CTwiddle, S> : k_line_ct<P, N, T, L, MINB, OpC2CTwiddle, S>;
       default: return nullptr;
     }
   } else if constexpr (ROWOPS) {
     switch (op) {
-      case OP_R2C: return k_line_ct<P, N, T, L, MINB, OpR2CPacked, S>;
-      case OP_C2R: return k_line_ct<P, N, T, L, MINB, OpC2RPacked, S>;
-      case OP_SPECTRO: return k_line_ct<P, N, T, L, MINB, OpSpectro, S>;
+      case OP_R2C:
+        return pipe ? k_line_pp<P, N, T, L, MINB, OpR2CPacked, S> : k_line_ct<P, N, T, L, MINB, OpR2CPacked, S>;
+      case OP_C2R:
+        return pipe ? k_line_pp<P, N, T, L, MINB, OpC2RPacked, S> : k_line_ct<P, N, T, L, MINB, OpC2RPacked, S>;
+      case OP_SPECTRO: return pipe ? nullptr : k_line_ct<P, N, T, L, MINB, OpSpectro, S>;
       default: return nullptr;
     }
   } else {
@@ -85,10 +89,10 @@ template <class P, int GROUP, int N, int T, int L, bool ROWOPS, int... Rs> KFn c
   }
 }
 
-template <class P, int GROUP> KFn pick_ct(int n, int T, int lpc, int op, const int *rad, int nst) {
+template <class P, int GROUP> KFn pick_ct(int n, int T, int lpc, int op, const int *rad, int nst, bool pipe) {
 #define GF_CT_X(N, TT, L, ROW, ...)                                           \
   if (n == N && T == TT && lpc == L && sched_eq<__VA_ARGS__>(rad, nst))      \
-    return ct_for<P, GROUP, N, TT, L, ROW != 0, __VA_ARGS__>(op);
+    return ct_for<P, GROUP, N, TT, L, ROW != 0, __VA_ARGS__>(op, pipe);
   GF_CT_LIST(GF_CT_X)
 #undef GF_CT_X
   return nullptr;
@@ -186,8 +190,9 @@ static inline int ew_blocks(long long total) {
 // translation units, so the build parallelises).
 #define GF_DEFINE_CT(P, SUFFIX, GROUP)                                                         \
   namespace gf {                                                                               \
-  KFn line_kernel_ct_##SUFFIX##_##GROUP(int n, int T, int lpc, int op, const int *rad, int nst) { \
-    return pick_ct<P, GROUP>(n, T, lpc, op, rad, nst);                                         \
+  KFn line_kernel_ct_##SUFFIX##_##GROUP(int n, int T, int lpc, int op, const int *rad, int nst,   \
+                                        bool pipe) {                                           \
+    return pick_ct<P, GROUP>(n, T, lpc, op, rad, nst, pipe);                                   \
   }                                                                                            \
   }
 

@@ -79,6 +79,62 @@ __global__ void __launch_bounds__(LPC *T, MINB) k_line_ct(const KArgs a) {
   if (!last_g) Op::template store<P>(a, line0);
 }
 
+
+// ---------------------------------------------------------------------------
+// Persistent, double-buffered variant: each CTA walks tiles (lpc lines)
+// blockIdx.x, blockIdx.x + gridDim.x, ...  While a tile is transformed in one
+// shared buffer, the asynchronous copies of the CTA's next tile fill the
+// other, so global-memory latency overlaps the butterflies.  The first stage
+// reads shared memory; the last stage writes global memory directly when the
+// op and layout allow.
+// ---------------------------------------------------------------------------
+GF_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+GF_DEV void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+GF_DEV void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <class P, int N, int T, int LPC, int MINB, class Op, class S>
+__global__ void __launch_bounds__(LPC *T, MINB) k_line_pp(const KArgs a) {
+  using C = typename P::cpx;
+  const long long ntiles = (a.nlines + LPC - 1) / LPC;
+  long long tile = blockIdx.x;
+  if (tile >= ntiles) return;
+  C *bufs[2] = {smem_base<C>(), smem_base<C>() + (size_t)LPC * spad_size(N)};
+  LineCtx c;
+  if (a.flags & GF_COLMAP) {
+    c.l = threadIdx.x % LPC;
+    c.t = threadIdx.x / LPC;
+  } else {
+    c.l = threadIdx.x / T;
+    c.t = threadIdx.x % T;
+  }
+  c.ioff = 0;
+  const bool last_g = Op::kTG && (a.flags & GF_LAST_DIRECT);
+  Op::template load<P>(a, tile * LPC, bufs[0]);
+  cp_async_commit();
+  int cur = 0;
+  for (; tile < ntiles; tile += gridDim.x) {
+    const long long next = tile + gridDim.x;
+    if (next < ntiles) {
+      Op::template load<P>(a, next * LPC, bufs[cur ^ 1]);
+      cp_async_commit();
+      cp_async_wait1();
+    } else {
+      cp_async_wait0();
+    }
+    __syncthreads();
+    const long long line0 = tile * LPC;
+    Op::template prep<P>(a, line0, bufs[cur]);
+    c.line = line0 + c.l;
+    c.valid = c.line < a.nlines;
+    c.ooff = c.valid ? line_off(a.out, (uint32_t)c.line) : 0;
+    const LineView<C> s = line_view<C>(a, c.l, bufs[cur]);
+    run_stages_ct<P, Op, N, T, false, Op::kTG>(S{}, s, a, c, Op::first_conj(a), false, last_g);
+    if (!last_g) Op::template store<P>(a, line0, bufs[cur]);
+    __syncthreads();
+    cur ^= 1;
+  }
+}
+
 // ===========================================================================
 // Table generation (FP64 on the device; exact integer angle reduction).
 // ===========================================================================

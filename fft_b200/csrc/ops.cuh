@@ -48,13 +48,13 @@ template <class P> GF_DEV void load_real_pair(const KArgs &a, Cx<P> *dst, long l
 
 // Copies bins 0..min(nb, cnt)-1 of each line raw into slots 0.., zeroing the
 // slots of missing bins up to cnt.
-template <class P> GF_DEV void load_bins(const KArgs &a, long long line0, int cnt, int nb) {
+template <class P> GF_DEV void load_bins(const KArgs &a, long long line0, int cnt, int nb, void *sb) {
   using C = Cx<P>;
   using Rl = typename P::real;
   const C *in = (const C *)a.in.ptr;
   tile_loop(a.in, a.lpc, cnt, FastDiv((uint32_t)cnt), a.lpcdiv, line0, a.nlines,
             [&](int l, int k, long long off) {
-              C *d = &line_view<C>(a, l)[k];
+              C *d = &line_view<C>(a, l, sb)[k];
               if (k < nb) cp_async_n<sizeof(C)>(d, &in[off]);
               else *d = mkc((Rl)0, (Rl)0);
             });
@@ -77,22 +77,22 @@ struct OpC2C {
     const Rl sc = (Rl)a.scale;
     ((Cx<P> *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = mkc(y.x * sc, y.y * (a.cj_out ? -sc : sc));
   }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     const C *in = (const C *)a.in.ptr;
     tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      cp_async_n<sizeof(C)>(&line_view<C>(a, l)[i], &in[off]);
+      cp_async_n<sizeof(C)>(&line_view<C>(a, l, sb)[i], &in[off]);
     });
   }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     using Rl = typename P::real;
     C *out = (C *)a.out.ptr;
     const Rl sc = (Rl)a.scale;
     const Rl sy = a.cj_out ? -sc : sc;
     tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      C y = line_view<C>(a, l)[i];
+      C y = line_view<C>(a, l, sb)[i];
       out[off] = mkc(y.x * sc, y.y * sy);
     });
   }
@@ -117,13 +117,13 @@ struct OpC2CTwiddle {
     if (!c.valid) return;
     ((Cx<P> *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = tw<P>(a, c.line, i, y);
   }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) { OpC2C::load<P>(a, line0); }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) { OpC2C::load<P>(a, line0, sb); }
+  template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     C *out = (C *)a.out.ptr;
     tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      out[off] = tw<P>(a, line0 + l, i, line_view<C>(a, l)[i]);
+      out[off] = tw<P>(a, line0 + l, i, line_view<C>(a, l, sb)[i]);
     });
   }
 };
@@ -136,7 +136,7 @@ struct OpC2CTwiddle {
 // input and complex bins on output.
 // ---------------------------------------------------------------------------
 template <class P, class F>
-GF_DEV void untangle_tile(const KArgs &a, long long line0, F emit) {
+GF_DEV void untangle_tile(const KArgs &a, long long line0, F emit, void *sb) {
   using C = Cx<P>;
   using Rl = typename P::real;
   using TW = typename P::tw_t;
@@ -146,7 +146,7 @@ GF_DEV void untangle_tile(const KArgs &a, long long line0, F emit) {
   const Rl half = (Rl)0.5;
   tile_loop(a.out, a.lpc, h, FastDiv((uint32_t)h), a.lpcdiv, line0, a.nlines,
             [&](int l, int k, long long off) {
-              const LineView<C> s = line_view<C>(a, l);
+              const LineView<C> s = line_view<C>(a, l, sb);
               const long long base = off - (long long)k * a.out.stride;
               if (k == 0) {
                 C z0 = s[0];
@@ -172,18 +172,18 @@ struct OpR2CPacked {
     return read_pair<P>(a, c.ioff + 2LL * j * a.in.stride, a.in.stride);
   }
   template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     const long long st = a.in.stride;
     tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
       const long long base = off - (long long)j * st + 2LL * j * st;
-      load_real_pair<P>(a, &line_view<Cx<P>>(a, l)[j], base, st);
+      load_real_pair<P>(a, &line_view<Cx<P>>(a, l, sb)[j], base, st);
     });
   }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
     Cx<P> *out = (Cx<P> *)a.out.ptr;
     const long long st = a.out.stride;
-    untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) { out[base + (long long)k * st] = v; });
+    untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) { out[base + (long long)k * st] = v; }, sb);
   }
 };
 
@@ -209,11 +209,11 @@ struct OpC2RPacked {
       out[base + st] = -y.y * sc;
     }
   }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     const int m = a.lp.n;
-    load_bins<P>(a, line0, m + 1, a.ic & GF_IC_MASK);
+    load_bins<P>(a, line0, m + 1, a.ic & GF_IC_MASK, sb);
   }
-  template <class P> static GF_DEV void prep(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void prep(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     using Rl = typename P::real;
     using TW = typename P::tw_t;
@@ -225,7 +225,7 @@ struct OpC2RPacked {
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       const int l = e / h, k = e - l * h;
       if (line0 + l >= a.nlines) continue;
-      const LineView<C> s = line_view<C>(a, l);
+      const LineView<C> s = line_view<C>(a, l, sb);
       if (k == 0) {
         const Rl x0 = s[0].x, xm = s[m].x;
         // Z[0] = ((x0+xm) + i(x0-xm))/2, stored conjugated
@@ -243,14 +243,14 @@ struct OpC2RPacked {
     }
     __syncthreads();
   }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     using Rl = typename P::real;
     Rl *out = (Rl *)a.out.ptr;
     const Rl sc = (Rl)a.scale;
     const long long st = a.out.stride;
     tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
-      C y = line_view<C>(a, l)[j];
+      C y = line_view<C>(a, l, sb)[j];
       const long long base = off - (long long)j * st + 2LL * j * st;
       out[base] = y.x * sc;
       out[base + st] = -y.y * sc;
@@ -272,22 +272,22 @@ struct OpR2CFull {
     if (!c.valid || i > a.lp.n / 2) return;
     ((Cx<P> *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = y;
   }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     using Rl = typename P::real;
     const Rl *in = (const Rl *)a.in.ptr;
     tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      Cx<P> *d = &line_view<Cx<P>>(a, l)[i];
+      Cx<P> *d = &line_view<Cx<P>>(a, l, sb)[i];
       cp_async_n<sizeof(Rl)>(&d->x, &in[off]);
       d->y = (Rl)0;
     });
   }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     C *out = (C *)a.out.ptr;
     const int h = a.lp.n / 2 + 1;
     tile_loop(a.out, a.lpc, h, FastDiv((uint32_t)h), a.lpcdiv, line0, a.nlines,
-              [&](int l, int k, long long off) { out[off] = line_view<C>(a, l)[k]; });
+              [&](int l, int k, long long off) { out[off] = line_view<C>(a, l, sb)[k]; });
   }
 };
 
@@ -303,33 +303,33 @@ struct OpC2RFull {
     if (!c.valid) return;
     ((Rl *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = y.x * (Rl)a.scale;
   }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
-    load_bins<P>(a, line0, a.lp.n / 2 + 1, a.ic & GF_IC_MASK);
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
+    load_bins<P>(a, line0, a.lp.n / 2 + 1, a.ic & GF_IC_MASK, sb);
   }
-  template <class P> static GF_DEV void prep(const KArgs &a, long long) {
+  template <class P> static GF_DEV void prep(const KArgs &a, long long, void *sb = nullptr) {
     using C = Cx<P>;
     const int n = a.lp.n;
     const int h = n / 2 + 1;
     const int up = n - h;  // mirrored elements i = h .. n-1
     for (int e = threadIdx.x; e < a.lpc * up; e += blockDim.x) {
       const int l = e / up, i = h + (e - l * up);
-      const LineView<C> s = line_view<C>(a, l);
+      const LineView<C> s = line_view<C>(a, l, sb);
       s[i] = s[n - i];  // conj(conj(bin(n-i)))
     }
     __syncthreads();
     for (int e = threadIdx.x; e < a.lpc * h; e += blockDim.x) {
       const int l = e / h, i = e - l * h;
-      const LineView<C> s = line_view<C>(a, l);
+      const LineView<C> s = line_view<C>(a, l, sb);
       s[i].y = -s[i].y;
     }
     __syncthreads();
   }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
     using Rl = typename P::real;
     Rl *out = (Rl *)a.out.ptr;
     const Rl sc = (Rl)a.scale;
     tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
-      out[off] = line_view<Cx<P>>(a, l)[i].x * sc;
+      out[off] = line_view<Cx<P>>(a, l, sb)[i].x * sc;
     });
   }
 };
@@ -372,7 +372,7 @@ struct OpRader {
     const long long d = __ldg(&((const int *)a.aux1)[qi]);
     ((C *)a.out.ptr)[c.ooff + d * a.out.stride] = mkc(v.x * sc, v.y * (a.cj_out ? -sc : sc));
   }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     using Rl = typename P::real;
     const C *in = (const C *)a.in.ptr;
@@ -382,7 +382,7 @@ struct OpRader {
     const long long st = a.in.stride;
     tile_loop(a.in, a.lpc, cl, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int k, long long off) {
       const long long base = off - (long long)k * st;
-      C *d = &line_view<C>(a, l)[k];
+      C *d = &line_view<C>(a, l, sb)[k];
       if (k < q) cp_async_n<sizeof(C)>(d, &in[base + (long long)__ldg(&perm[k]) * st]);
       else *d = mkc((Rl)0, (Rl)0);
       if (k == 0) {
@@ -392,8 +392,8 @@ struct OpRader {
       }
     });
   }
-  template <class P> static GF_DEV void prep(const KArgs &, long long) {}
-  template <class P> static GF_DEV void mid(const KArgs &a, long long line0, bool last_g) {
+  template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
+  template <class P> static GF_DEV void mid(const KArgs &a, long long line0, bool last_g, void *sb = nullptr) {
     using C = Cx<P>;
     using Rl = typename P::real;
     using SP = typename P::sp_t;
@@ -402,7 +402,7 @@ struct OpRader {
     // X[0] first (reads A[0] before the multiply overwrites it)
     for (int l = threadIdx.x; l < a.lpc; l += blockDim.x) {
       C *ex = line_extra<C>(a, l);
-      ex[1] = cadd(ex[0], line_view<C>(a, l)[0]);
+      ex[1] = cadd(ex[0], line_view<C>(a, l, sb)[0]);
       if (last_g && line0 + l < a.nlines) {
         const Rl sc = (Rl)a.scale;
         ((C *)a.out.ptr)[line_off(a.out, (uint32_t)(line0 + l))] =
@@ -414,12 +414,12 @@ struct OpRader {
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       uint32_t l, k;
       a.ndiv.divmod((uint32_t)e, l, k);
-      const LineView<C> s = line_view<C>(a, (int)l);
+      const LineView<C> s = line_view<C>(a, (int)l, sb);
       s[k] = cconj(spmul(s[k], __ldg(&B[k])));
     }
     __syncthreads();
   }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     using Rl = typename P::real;
     C *out = (C *)a.out.ptr;
@@ -439,7 +439,7 @@ struct OpRader {
                   y = ex[1];
                   dst = 0;
                 } else {
-                  y = cadd(ex[0], cconj(line_view<C>(a, l)[i - 1 + offc]));
+                  y = cadd(ex[0], cconj(line_view<C>(a, l, sb)[i - 1 + offc]));
                   dst = __ldg(&iperm[i - 1]);
                 }
                 out[base + dst * st] = mkc(y.x * sc, y.y * sy);
@@ -475,33 +475,33 @@ struct OpBluestein {
     const Rl sc = (Rl)a.scale;
     ((C *)a.out.ptr)[c.ooff + (long long)k * a.out.stride] = mkc(v.x * sc, v.y * (a.cj_out ? -sc : sc));
   }
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     using Rl = typename P::real;
     const C *in = (const C *)a.in.ptr;
     const int n = (int)a.ia;
     tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
-      C *d = &line_view<C>(a, l)[j];
+      C *d = &line_view<C>(a, l, sb)[j];
       if (j < n) cp_async_n<sizeof(C)>(d, &in[off]);
       else *d = mkc((Rl)0, (Rl)0);
     });
   }
   // a[j] = conj?(x[j]) * w[j] for j < n
-  template <class P> static GF_DEV void prep(const KArgs &a, long long) {
+  template <class P> static GF_DEV void prep(const KArgs &a, long long, void *sb = nullptr) {
     using C = Cx<P>;
     using SP = typename P::sp_t;
     const SP *w = (const SP *)a.aux0;
     const int n = (int)a.ia;
     for (int e = threadIdx.x; e < a.lpc * n; e += blockDim.x) {
       const int l = e / n, j = e - l * n;
-      const LineView<C> s = line_view<C>(a, l);
+      const LineView<C> s = line_view<C>(a, l, sb);
       C v = s[j];
       if (a.cj_in) v.y = -v.y;
       s[j] = spmul(v, __ldg(&w[j]));
     }
     __syncthreads();
   }
-  template <class P> static GF_DEV void mid(const KArgs &a, long long, bool) {
+  template <class P> static GF_DEV void mid(const KArgs &a, long long, bool, void *sb = nullptr) {
     using C = Cx<P>;
     using SP = typename P::sp_t;
     const SP *B = (const SP *)a.aux2;
@@ -509,12 +509,12 @@ struct OpBluestein {
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       uint32_t l, k;
       a.ndiv.divmod((uint32_t)e, l, k);
-      const LineView<C> s = line_view<C>(a, (int)l);
+      const LineView<C> s = line_view<C>(a, (int)l, sb);
       s[k] = cconj(spmul(s[k], __ldg(&B[k])));
     }
     __syncthreads();
   }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
     using Rl = typename P::real;
     using SP = typename P::sp_t;
@@ -525,7 +525,7 @@ struct OpBluestein {
     const Rl sy = a.cj_out ? -sc : sc;
     tile_loop(a.out, a.lpc, n, FastDiv((uint32_t)n), a.lpcdiv, line0, a.nlines,
               [&](int l, int k, long long off) {
-                C y = spmul(cconj(line_view<C>(a, l)[k]), __ldg(&w[k]));
+                C y = spmul(cconj(line_view<C>(a, l, sb)[k]), __ldg(&w[k]));
                 out[off] = mkc(y.x * sc, y.y * sy);
               });
   }
@@ -550,27 +550,27 @@ struct OpSpectro {
     return mkc(v.x * __ldg(&win[2 * j]), v.y * __ldg(&win[2 * j + 1]));
   }
   template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
-  template <class P> static GF_DEV void load(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     tile_loop(a.in, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int j, long long off) {
       // stride 1: complex element j sits at off = line + j; its real pair is
       // at line + 2j = off + j
-      load_real_pair<P>(a, &line_view<Cx<P>>(a, l)[j], off + j, 1);
+      load_real_pair<P>(a, &line_view<Cx<P>>(a, l, sb)[j], off + j, 1);
     });
   }
-  template <class P> static GF_DEV void prep(const KArgs &a, long long) {
+  template <class P> static GF_DEV void prep(const KArgs &a, long long, void *sb = nullptr) {
     using C = Cx<P>;
     using Rl = typename P::real;
     const Rl *win = (const Rl *)a.aux1;
     const int m = a.lp.n;
     for (int e = threadIdx.x; e < a.lpc * m; e += blockDim.x) {
       const int l = e / m, j = e - l * m;
-      const LineView<C> s = line_view<C>(a, l);
+      const LineView<C> s = line_view<C>(a, l, sb);
       C v = s[j];
       s[j] = mkc(v.x * __ldg(&win[2 * j]), v.y * __ldg(&win[2 * j + 1]));
     }
     __syncthreads();
   }
-  template <class P> static GF_DEV void store(const KArgs &a, long long line0) {
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
     using Rl = typename P::real;
     Rl *out = (Rl *)a.out.ptr;
     const Rl sc = (Rl)a.scale;
@@ -579,7 +579,7 @@ struct OpSpectro {
       Rl pw = (v.x * v.x + v.y * v.y) * sc;
       if (k != 0 && k != m) pw *= (Rl)2;
       out[base + k] = pw;
-    });
+    }, sb);
   }
 };
 

@@ -155,15 +155,30 @@ static KFn kernel_for(int prec, int maxe, int op) {
   }
 }
 
-static KFn kernel_ct_for(const DevProg &dp, int op, int lpc) {
+static KFn kernel_ct_for(const DevProg &dp, int op, int lpc, bool pipe) {
   const bool g0 = op == OP_C2C || op == OP_C2C_TW;
   const int n = dp.n, T = dp.lp.T, nst = dp.lp.nst;
   const int *r = dp.lp.radix;
   switch (dp.prec) {
-    case F64: return g0 ? line_kernel_ct_f64_0(n, T, lpc, op, r, nst) : line_kernel_ct_f64_1(n, T, lpc, op, r, nst);
-    case F32: return g0 ? line_kernel_ct_f32_0(n, T, lpc, op, r, nst) : line_kernel_ct_f32_1(n, T, lpc, op, r, nst);
-    default: return g0 ? line_kernel_ct_f32c_0(n, T, lpc, op, r, nst) : line_kernel_ct_f32c_1(n, T, lpc, op, r, nst);
+    case F64:
+      return g0 ? line_kernel_ct_f64_0(n, T, lpc, op, r, nst, pipe) : line_kernel_ct_f64_1(n, T, lpc, op, r, nst, pipe);
+    case F32:
+      return g0 ? line_kernel_ct_f32_0(n, T, lpc, op, r, nst, pipe) : line_kernel_ct_f32_1(n, T, lpc, op, r, nst, pipe);
+    default:
+      return g0 ? line_kernel_ct_f32c_0(n, T, lpc, op, r, nst, pipe)
+                : line_kernel_ct_f32c_1(n, T, lpc, op, r, nst, pipe);
   }
+}
+
+static int num_sms() {
+  static int v = 0;
+  if (!v) {
+    int d = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+    if (v <= 0) v = 148;
+  }
+  return v;
 }
 
 static int ensure_smem(KFn f, size_t smem) {
@@ -457,10 +472,27 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   if (const char *e = getenv("GOFFT_NO_DIRECT")) {
     if (*e == '1') a.flags &= GF_COLMAP;
   }
-  const size_t smem = (size_t)lpc * spad_size(dp.n) * csize(dp.prec) + (conv ? 2 * lpc * csize(dp.prec) : 0);
+  size_t smem = (size_t)lpc * spad_size(dp.n) * csize(dp.prec) + (conv ? 2 * lpc * csize(dp.prec) : 0);
   KFn f = nullptr;
   static const bool no_ct = getenv("GOFFT_NO_CT") && getenv("GOFFT_NO_CT")[0] == '1';
-  if (!conv && !no_ct) f = kernel_ct_for(dp, op, lpc);
+  static const bool no_pipe = getenv("GOFFT_NO_PIPE") && getenv("GOFFT_NO_PIPE")[0] == '1';
+  long long grid = (nlines + lpc - 1) / lpc;
+  if (!conv && !no_ct) {
+    // persistent double-buffered variant when two tile buffers fit
+    if (!no_pipe && 2 * smem <= max_smem_optin() && grid > 2 * num_sms()) {
+      f = kernel_ct_for(dp, op, lpc, true);
+      if (f) {
+        if (int rc = ensure_smem(f, 2 * smem)) return rc;
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)f, lpc * dp.lp.T, 2 * smem);
+        if (per_sm < 1) per_sm = 1;
+        grid = std::min<long long>(grid, (long long)per_sm * num_sms());
+        smem *= 2;
+        a.flags &= ~GF_FIRST_DIRECT;
+      }
+    }
+    if (!f) f = kernel_ct_for(dp, op, lpc, false);
+  }
   if (!f) {
     // the run-time-schedule kernel has no direct stages
     f = kernel_for(dp.prec, dp.maxe, op);
@@ -468,7 +500,6 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   }
   if (!f) return set_err(5, "no kernel instance for this precision/op");
   if (int rc = ensure_smem(f, smem)) return rc;
-  const long long grid = (nlines + lpc - 1) / lpc;
   count_launch();
   TimingRec rec;
   const bool timed = g_timing.load() != 0;
