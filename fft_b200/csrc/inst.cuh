@@ -61,11 +61,18 @@ template <int... Rs> constexpr bool sched_eq(const int *r, int nst) {
   return true;
 }
 
+#ifndef GF_F32_MINB
+#define GF_F32_MINB 3
+#endif
+
 // GROUP 0: complex ops (C2C, four-step twiddle); GROUP 1: real-row ops.
 // PIPE selects the persistent double-buffered kernel.
 template <class P, int GROUP, int N, int T, int L, bool ROWOPS, int... Rs> KFn ct_for(int op, bool pipe) {
   using S = Sched<Rs...>;
-  constexpr int MINB = (L * T <= 256) ? 2 : 1;
+  // FP64 butterflies need ~128 registers (two 256-thread CTAs per SM); the
+  // FP32 forms fit in fewer, so ask for more resident CTAs (more warps to
+  // hide shared-memory and twiddle latency).
+  constexpr int MINB = (L * T <= 256) ? (sizeof(typename P::cpx) == 16 ? 2 : GF_F32_MINB) : 1;
   if constexpr (N == 16384 && sizeof(typename P::cpx) == 16) {
     return nullptr;  // FP64 16384 is two-pass
   } else if constexpr (GROUP == 0) {
