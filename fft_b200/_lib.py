@@ -65,6 +65,7 @@ SIGNATURES = {
     "gofft_timing_enable": (ctypes.c_int, [ctypes.c_int]),
     "gofft_timing_report": (_i64, [ctypes.c_char_p, _i64]),
     "gofft_set_lines_per_cta": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "gofft_set_pipelined": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int]),
 }
 
 _lib = None

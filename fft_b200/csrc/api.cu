@@ -132,7 +132,9 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       // images per block: keep a block's complex intermediate L2-resident
       const long long budget = env_ll("GOFFT_L2_BLOCK_BYTES", 48ll << 20);
       const long long per = p->shape[0] * rc * (long long)csize(precision);
-      p->chunk = std::max<long long>(1, std::min<long long>(batch, budget / std::max<long long>(1, per)));
+      const long long cmax = std::max<long long>(1, std::min<long long>(batch, budget / std::max<long long>(1, per)));
+      const long long nblocks = (batch + cmax - 1) / cmax;
+      p->chunk = (batch + nblocks - 1) / nblocks;  // balanced blocks
     }
   }
   if (int rc2 = plan_ws(p.get())) return rc2;
@@ -736,5 +738,9 @@ extern "C" int64_t gofft_timing_report(char *buf, int64_t cap) {
 }
 extern "C" int gofft_set_lines_per_cta(int precision, int64_t n, int op, int colmode, int lpc) {
   set_lpc_override(precision, n, op, colmode, lpc);
+  return GOFFT_OK;
+}
+extern "C" int gofft_set_pipelined(int precision, int64_t n, int op, int on) {
+  set_pipe_override(precision, n, op, on);
   return GOFFT_OK;
 }

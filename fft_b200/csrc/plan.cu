@@ -386,6 +386,16 @@ static double algo_bytes(int op, const DevProg &dp, const KArgs &a, long long nl
 // ---------------------------------------------------------------------------
 static std::mutex g_lpc_mu;
 static std::map<std::tuple<int, long long, int, int>, int> g_lpc;
+static std::map<std::tuple<int, long long, int>, int> g_pipe;
+void set_pipe_override(int prec, long long n, int op, int on) {
+  std::lock_guard<std::mutex> lk(g_lpc_mu);
+  g_pipe[std::make_tuple(prec, n, op)] = on;
+}
+int get_pipe_override(int prec, long long n, int op) {
+  std::lock_guard<std::mutex> lk(g_lpc_mu);
+  auto it = g_pipe.find(std::make_tuple(prec, n, op));
+  return it == g_pipe.end() ? 0 : it->second;
+}
 void set_lpc_override(int prec, long long n, int op, int colmode, int lpc) {
   std::lock_guard<std::mutex> lk(g_lpc_mu);
   if (lpc <= 0) g_lpc.erase(std::make_tuple(prec, n, op, colmode));
@@ -475,7 +485,11 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   size_t smem = (size_t)lpc * spad_size(dp.n) * csize(dp.prec) + (conv ? 2 * lpc * csize(dp.prec) : 0);
   KFn f = nullptr;
   static const bool no_ct = getenv("GOFFT_NO_CT") && getenv("GOFFT_NO_CT")[0] == '1';
-  static const bool no_pipe = getenv("GOFFT_NO_PIPE") && getenv("GOFFT_NO_PIPE")[0] == '1';
+  // the persistent double-buffered variant halves resident CTAs; measured
+  // slower on the 1024/512-point lines, so it is opt-in (GOFFT_PIPE=1 or the
+  // autotuner's pipe choice)
+  static const bool env_pipe = getenv("GOFFT_PIPE") && getenv("GOFFT_PIPE")[0] == '1';
+  const bool no_pipe = !(env_pipe || get_pipe_override(dp.prec, dp.n, op));
   long long grid = (nlines + lpc - 1) / lpc;
   if (!conv && !no_ct) {
     // persistent double-buffered variant when two tile buffers fit

@@ -124,5 +124,7 @@ std::string timing_report();
 // Autotuned lines-per-CTA overrides (key: prec, n, op, column-mode).
 void set_lpc_override(int prec, long long n, int op, int colmode, int lpc);
 int get_lpc_override(int prec, long long n, int op, int colmode);
+void set_pipe_override(int prec, long long n, int op, int on);
+int get_pipe_override(int prec, long long n, int op);
 
 }  // namespace gf

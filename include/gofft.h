@@ -193,6 +193,9 @@ GOFFT_API int64_t gofft_timing_report(char *buf, int64_t cap);
 /* Overrides the lines-per-CTA of the line kernel for (precision, length n,
  * op, column mode); lpc <= 0 restores the heuristic.  Used by the autotuner. */
 GOFFT_API int gofft_set_lines_per_cta(int precision, int64_t n, int op, int colmode, int lpc);
+/* Selects (on = 1) the persistent double-buffered line kernel for
+ * (precision, n, op) where one exists.  Used by the autotuner. */
+GOFFT_API int gofft_set_pipelined(int precision, int64_t n, int op, int on);
 
 #ifdef __cplusplus
 }
