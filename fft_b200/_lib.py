@@ -61,6 +61,16 @@ SIGNATURES = {
     "gofft_plan_table": (_i64, [_vp, ctypes.c_int, _i64p, _i64]),
     "gofft_spectrogram_device": (ctypes.c_int, [ctypes.c_int, _vp, _i64, _i64, _i64, _vp, ctypes.c_double, _vp,
                                                 _i64p, _vp]),
+    "gofft_uneven_create": (ctypes.c_int, [ctypes.c_int, _i64p, _i64, _i64p, _i64p, _pp]),
+    "gofft_uneven_destroy": (ctypes.c_int, [_vp]),
+    "gofft_uneven_exec": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
+    "gofft_uneven_status": (ctypes.c_int, [_vp]),
+    "gofft_uneven_set": (ctypes.c_int, [_vp, ctypes.c_int, _i64]),
+    "gofft_uneven_describe": (_i64, [_vp, ctypes.c_char_p, _i64]),
+    "gofft_graph_begin": (ctypes.c_int, [_vp]),
+    "gofft_graph_end": (ctypes.c_int, [_vp, _pp]),
+    "gofft_graph_launch": (ctypes.c_int, [_vp, _vp]),
+    "gofft_graph_destroy": (ctypes.c_int, [_vp]),
     "gofft_launch_count": (_i64, []),
     "gofft_timing_enable": (ctypes.c_int, [ctypes.c_int]),
     "gofft_timing_report": (_i64, [ctypes.c_char_p, _i64]),

@@ -744,3 +744,38 @@ extern "C" int gofft_set_pipelined(int precision, int64_t n, int op, int on) {
   set_pipe_override(precision, n, op, on);
   return GOFFT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// CUDA graphs
+// ---------------------------------------------------------------------------
+struct gofft_graph {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+  ~gofft_graph() {
+    if (x) cudaGraphExecDestroy(x);
+    if (g) cudaGraphDestroy(g);
+  }
+};
+
+extern "C" int gofft_graph_begin(gofft_stream stream) {
+  if (!stream) return set_err(GOFFT_EINVAL, "capture needs a non-default stream");
+  GF_CK(cudaStreamBeginCapture((cudaStream_t)stream, cudaStreamCaptureModeThreadLocal));
+  return GOFFT_OK;
+}
+extern "C" int gofft_graph_end(gofft_stream stream, gofft_graph **out) {
+  if (!out) return set_err(GOFFT_EINVAL, "null output handle");
+  std::unique_ptr<gofft_graph> g(new gofft_graph());
+  GF_CK(cudaStreamEndCapture((cudaStream_t)stream, &g->g));
+  GF_CK(cudaGraphInstantiate(&g->x, g->g, 0));
+  *out = g.release();
+  return GOFFT_OK;
+}
+extern "C" int gofft_graph_launch(gofft_graph *g, gofft_stream stream) {
+  if (!g) return set_err(GOFFT_EINVAL, "null graph");
+  GF_CK(cudaGraphLaunch(g->x, (cudaStream_t)stream));
+  return GOFFT_OK;
+}
+extern "C" int gofft_graph_destroy(gofft_graph *g) {
+  delete g;
+  return GOFFT_OK;
+}

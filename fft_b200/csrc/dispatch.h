@@ -16,7 +16,10 @@ enum Op {
   OP_RADER = 6,    // fused Rader convolution
   OP_BLUE = 7,     // fused Bluestein convolution
   OP_SPECTRO = 8,  // fused spectrogram frame
-  OP_COUNT = 9
+  OP_RADER_FS1 = 9,   // two-pass Rader: gathered column pass
+  OP_RADER_FS2 = 10,  // two-pass Rader: row pass with spectrum multiply
+  OP_RADER_FS4 = 11,  // two-pass Rader: row pass with the output scatter
+  OP_COUNT = 12
 };
 
 typedef void (*KFn)(KArgs);

@@ -46,17 +46,25 @@ struct LineProg {
 };
 
 // Addressing of one side of a batched, strided set of lines (in elements).
-// line l, element i:  (l / lpb) * dist_b + (l % lpb) * dist_l + i * stride.
+// line l, element i:  base(l / lpb) + (l % lpb) * dist_l + i * stride, with
+// base(b) = b * dist_b, or boff[b] when a per-batch offset table is given
+// (signals of one length scattered through an uneven batch).
 struct Side {
   void *ptr;
   long long dist_b, dist_l, stride;
   FastDiv lpb;
+  const long long *boff;
 };
 
 GF_HD long long line_off(const Side &s, uint32_t l) {
   uint32_t b, r;
   s.lpb.divmod(l, b, r);
-  return (long long)b * s.dist_b + (long long)r * s.dist_l;
+#ifdef __CUDA_ARCH__
+  const long long base = s.boff ? __ldg(&s.boff[b]) : (long long)b * s.dist_b;
+#else
+  const long long base = s.boff ? s.boff[b] : (long long)b * s.dist_b;
+#endif
+  return base + (long long)r * s.dist_l;
 }
 
 // Stage layout used to generate the twiddle planes of a LineProg.

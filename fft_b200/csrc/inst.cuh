@@ -14,6 +14,9 @@ template <class P, int M, int GROUP> KFn pick_line(int op) {
       case OP_C2C_TW: return k_line<P, M, OpC2CTwiddle>;
       case OP_RADER: return k_line<P, M, OpRader>;
       case OP_BLUE: return k_line<P, M, OpBluestein>;
+      case OP_RADER_FS1: return k_line<P, M, OpRaderFS1>;
+      case OP_RADER_FS2: return k_line<P, M, OpRaderFS2>;
+      case OP_RADER_FS4: return k_line<P, M, OpRaderFS4>;
       default: return nullptr;
     }
   } else {

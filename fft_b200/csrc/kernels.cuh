@@ -2,6 +2,7 @@
 // multi-pass plans and plan construction (twiddle and spectrum tables).
 #pragma once
 #include <type_traits>
+#include "dispatch.h"
 #include "ops.cuh"
 
 namespace gf {
@@ -12,14 +13,18 @@ namespace gf {
 // (GF_COLMAP); the first / last stage read / write global memory directly
 // when the op supports it and the host set GF_FIRST_DIRECT / GF_LAST_DIRECT.
 // ---------------------------------------------------------------------------
+// One tile (lines tile*lpc ..) of a run-time-schedule line op.  Threads at or
+// beyond lpc*T (a persistent kernel sized for a larger op) only take part in
+// the barriers and the cooperative tile loops.
 template <class P, int MAXE, class Op>
-__global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
-  // The run-time-schedule kernel always uses the tile prologue / epilogue:
-  // direct stages would multiply its (already long) body by four.
+GF_DEV void line_body(const KArgs &a, long long tile, bool active) {
   using C = typename P::cpx;
-  const long long line0 = (long long)blockIdx.x * a.lpc;
+  const long long line0 = tile * a.lpc;
   LineCtx c;
-  if (a.flags & GF_COLMAP) {
+  if (!active) {
+    c.l = 0;
+    c.t = 1 << 29;  // no butterflies
+  } else if (a.flags & GF_COLMAP) {
     c.l = threadIdx.x % a.lpc;
     c.t = threadIdx.x / a.lpc;
   } else {
@@ -27,7 +32,7 @@ __global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
     c.t = threadIdx.x - c.l * a.lp.T;
   }
   c.line = line0 + c.l;
-  c.valid = c.line < a.nlines;
+  c.valid = active && c.line < a.nlines;
   c.ioff = 0;
   c.ooff = 0;
   Op::template load<P>(a, line0);
@@ -43,6 +48,98 @@ __global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
     run_stages<P, Op, MAXE, false, false>(s, a, c, Op::first_conj(a), false, false);
   }
   Op::template store<P>(a, line0);
+}
+
+// The run-time-schedule kernel always uses the tile prologue / epilogue:
+// direct stages would multiply its (already long) body by four.
+template <class P, int MAXE, class Op>
+__global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
+  line_body<P, MAXE, Op>(a, blockIdx.x, true);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent multi-phase kernel (uneven batches).  A phase is one line op over
+// ntiles tiles; items (phase, tile) are numbered phase by phase and claimed
+// from a global counter.  A phase with a prerequisite waits until every tile
+// of that phase is done: its items come later in the numbering, so the
+// prerequisite's items were claimed by running CTAs that never wait on later
+// items, and the wait ends.  Each wait is bounded: past spin_limit polls the
+// CTA sets *err and carries on (results are then invalid and the host reports
+// a timeout).
+// ---------------------------------------------------------------------------
+struct PhaseDesc {
+  KArgs a;
+  int op;
+  int dep;           // prerequisite phase or -1
+  long long ntiles;
+  long long first;   // number of the phase's first item
+};
+
+template <class P>
+GF_DEV void phase_dispatch(const KArgs &a, int op, long long tile, bool active) {
+  switch (op) {
+    case OP_C2C: line_body<P, 16, OpC2C>(a, tile, active); break;
+    case OP_C2C_TW: line_body<P, 16, OpC2CTwiddle>(a, tile, active); break;
+    case OP_RADER: line_body<P, 16, OpRader>(a, tile, active); break;
+    case OP_BLUE: line_body<P, 16, OpBluestein>(a, tile, active); break;
+    case OP_RADER_FS1: line_body<P, 16, OpRaderFS1>(a, tile, active); break;
+    case OP_RADER_FS2: line_body<P, 16, OpRaderFS2>(a, tile, active); break;
+    case OP_RADER_FS4: line_body<P, 16, OpRaderFS4>(a, tile, active); break;
+    default: break;
+  }
+}
+
+template <class P>
+__global__ void __launch_bounds__(512, 1) k_persist(const PhaseDesc *ph, int nph, long long total,
+                                                     unsigned long long *ctr, int *done, int *err,
+                                                     long long spin_limit) {
+  __shared__ __align__(16) unsigned char sa_raw[sizeof(KArgs)];
+  KArgs &sa = *reinterpret_cast<KArgs *>(sa_raw);
+  __shared__ long long s_item;
+  __shared__ int s_p;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long it = (long long)atomicAdd(ctr, 1ull);
+      s_item = it;
+      if (it < total) {
+        int lo = 0, hi = nph - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) / 2;
+          if (ph[mid].first <= it) lo = mid;
+          else hi = mid - 1;
+        }
+        s_p = lo;
+        const int d = ph[lo].dep;
+        if (d >= 0) {
+          const int need = (int)ph[d].ntiles;
+          long long polls = 0;
+          while (*((volatile int *)&done[d]) < need) {
+            if (++polls > spin_limit) {
+              atomicExch(err, 1);
+              break;
+            }
+            __nanosleep(128);
+          }
+          __threadfence();
+        }
+      }
+    }
+    __syncthreads();
+    const long long item = s_item;
+    if (item >= total) break;
+    const int p = s_p;
+    {
+      const int *src = reinterpret_cast<const int *>(&ph[p].a);
+      int *dst = reinterpret_cast<int *>(&sa);
+      for (int i = threadIdx.x; i < (int)(sizeof(KArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const bool active = threadIdx.x < sa.lpc * sa.lp.T;
+    phase_dispatch<P>(sa, ph[p].op, item - ph[p].first, active);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&done[p], 1);
+  }
 }
 
 // ---------------------------------------------------------------------------

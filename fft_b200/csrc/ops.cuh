@@ -583,4 +583,130 @@ struct OpSpectro {
   }
 };
 
+
+// ---------------------------------------------------------------------------
+// Rader through a two-pass (four-step) convolution, for primes whose
+// convolution length cl = N1 * N2 does not fit one CTA.  Four line-kernel
+// phases per signal, all on the shared-memory prologue/epilogue:
+//   FS1  columns n2 of the conv signal a[n2 + N2 n1] = x[perm[..]] (zero past
+//        q), FFT over n1, twiddle W_cl^{n2 k1}; stashes x0 per signal
+//   FS2  rows k1, FFT over n2, output k = k1 + N1 k2 becomes conj(A[k] B[k]);
+//        records X[0] = x0 + A[0] per signal
+//   FS3  the plain twiddled column pass (OpC2CTwiddle) of the second FFT
+//   FS4  rows, FFT, and the scatter X[iperm[k - off]] = x0 + conj(v) for
+//        off <= k < off + q, plus X[0]
+// Signals of the phase are batches b; lines within a signal are the
+// sides' lpb groups.
+// ---------------------------------------------------------------------------
+struct OpRaderFS1 {  // aux0 perm, aux1 W_cl table, aux2 x0s; ia = cl, ib = q
+  static constexpr bool kConv = false, kFG = false, kTG = false;
+  static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &, const LineCtx &, int) { return Cx<P>(); }
+  template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    const C *in = (const C *)a.in.ptr;
+    const int *perm = (const int *)a.aux0;
+    const int q = (int)a.ib;
+    const int N2 = (int)a.in.lpb.d;
+    const int n1len = a.lp.n;
+    const int total = a.lpc * n1len;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int l = e / n1len, i = e - l * n1len;
+      const long long gl = line0 + l;
+      if (gl >= a.nlines) continue;
+      uint32_t b, n2;
+      a.in.lpb.divmod((uint32_t)gl, b, n2);
+      const long long base = line_off(a.in, (uint32_t)gl);  // signal base (dist_l = 0)
+      const int n = (int)n2 + N2 * i;
+      C *d = &line_view<C>(a, l, sb)[i];
+      if (n < q) cp_async_n<sizeof(C)>(d, &in[base + (long long)__ldg(&perm[n]) * a.in.stride]);
+      else *d = mkc((Rl)0, (Rl)0);
+      if (n == 0) {
+        C x0 = in[base];
+        if (a.cj_in) x0.y = -x0.y;
+        ((C *)a.aux2)[b] = x0;
+      }
+    }
+  }
+  template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
+    using C = Cx<P>;
+    using TW = typename P::tw_t;
+    C *out = (C *)a.out.ptr;
+    tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
+      uint32_t b, n2;
+      a.out.lpb.divmod((uint32_t)(line0 + l), b, n2);
+      const long long e = ((long long)n2 * i) % a.ia;
+      out[off] = twmul(line_view<C>(a, l, sb)[i], __ldg(&((const TW *)a.aux1)[e]));
+    });
+  }
+};
+
+struct OpRaderFS2 {  // aux0 B/cl spectrum, aux1 x0s, aux2 dc
+  static constexpr bool kConv = false, kFG = false, kTG = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &, const LineCtx &, int) { return Cx<P>(); }
+  template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
+    OpC2C::load<P>(a, line0, sb);
+  }
+  template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
+    using C = Cx<P>;
+    using SP = typename P::sp_t;
+    C *out = (C *)a.out.ptr;
+    const int N1 = (int)a.out.lpb.d;
+    tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int k2, long long off) {
+      uint32_t b, k1;
+      a.out.lpb.divmod((uint32_t)(line0 + l), b, k1);
+      const long long k = (long long)k1 + (long long)N1 * k2;
+      const C v = line_view<C>(a, l, sb)[k2];
+      if (k == 0) ((C *)a.aux2)[b] = cadd(((const C *)a.aux1)[b], v);
+      out[off] = cconj(spmul(v, __ldg(&((const SP *)a.aux0)[k])));
+    });
+  }
+};
+
+struct OpRaderFS4 {  // aux0 iperm, aux1 x0s, aux2 dc; ia = q, ib = off
+  static constexpr bool kConv = false, kFG = false, kTG = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &, const LineCtx &, int) { return Cx<P>(); }
+  template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
+    OpC2C::load<P>(a, line0, sb);
+  }
+  template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    C *out = (C *)a.out.ptr;
+    const int N1 = (int)a.out.lpb.d;
+    const int q = (int)a.ia;
+    const int offc = (int)a.ib;
+    const Rl sc = (Rl)a.scale;
+    const Rl sy = a.cj_out ? -sc : sc;
+    const int n2len = a.lp.n;
+    const int total = a.lpc * n2len;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int l = e / n2len, k2 = e - l * n2len;
+      const long long gl = line0 + l;
+      if (gl >= a.nlines) continue;
+      uint32_t b, k1;
+      a.out.lpb.divmod((uint32_t)gl, b, k1);
+      const long long base = line_off(a.out, (uint32_t)gl);  // signal base (dist_l = 0)
+      const long long k = (long long)k1 + (long long)N1 * k2;
+      if (k == 0) {
+        const C d = ((const C *)a.aux2)[b];
+        out[base] = mkc(d.x * sc, d.y * sy);
+      }
+      const long long qi = k - offc;
+      if (qi < 0 || qi >= q) continue;
+      const C y = cadd(((const C *)a.aux1)[b], cconj(line_view<C>(a, l, sb)[k2]));
+      out[base + (long long)__ldg(&((const int *)a.aux0)[qi]) * a.out.stride] = mkc(y.x * sc, y.y * sy);
+    }
+  }
+};
+
 }  // namespace gf

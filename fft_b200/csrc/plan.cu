@@ -147,7 +147,8 @@ static size_t max_smem_optin() {
 }
 
 static KFn kernel_for(int prec, int maxe, int op) {
-  const bool g0 = op == OP_C2C || op == OP_C2C_TW || op == OP_RADER || op == OP_BLUE;
+  const bool g0 = op == OP_C2C || op == OP_C2C_TW || op == OP_RADER || op == OP_BLUE || op == OP_RADER_FS1 ||
+                  op == OP_RADER_FS2 || op == OP_RADER_FS4;
   switch (prec) {
     case F64: return g0 ? line_kernel_f64_0(maxe, op) : line_kernel_f64_1(maxe, op);
     case F32: return g0 ? line_kernel_f32_0(maxe, op) : line_kernel_f32_1(maxe, op);
@@ -361,8 +362,9 @@ std::string timing_report() {
 }
 
 static const char *op_name(int op) {
-  static const char *n[] = {"c2c", "c2c_twiddle", "r2c_packed", "c2r_packed", "r2c_full",
-                            "c2r_full", "rader_fused", "bluestein_fused", "spectrogram"};
+  static const char *n[] = {"c2c", "c2c_twiddle", "r2c_packed", "c2r_packed", "r2c_full", "c2r_full",
+                            "rader_fused", "bluestein_fused", "spectrogram", "rader_fs1", "rader_fs2",
+                            "rader_fs4"};
   return (op >= 0 && op < OP_COUNT) ? n[op] : "?";
 }
 
@@ -407,7 +409,7 @@ int get_lpc_override(int prec, long long n, int op, int colmode) {
   return it == g_lpc.end() ? 0 : it->second;
 }
 
-static int choose_lpc(const DevProg &dp, const KArgs &a, int op, long long nlines, bool conv) {
+int choose_lpc(const DevProg &dp, const KArgs &a, int op, long long nlines, bool conv) {
   const int T = dp.lp.T;
   const size_t line_bytes = (size_t)spad_size(dp.n) * csize(dp.prec) + (conv ? 2 * csize(dp.prec) : 0);
   const size_t smax = max_smem_optin();
@@ -436,7 +438,7 @@ static int choose_lpc(const DevProg &dp, const KArgs &a, int op, long long nline
 // aligned to the pair size (so it moves as one vector copy).
 bool pairs_aligned(const Side &s, int prec) {
   const long long pb = 2 * (long long)rsize(prec);
-  return s.stride == 1 && ((uintptr_t)s.ptr % pb) == 0 && (s.dist_b % 2) == 0 &&
+  return s.stride == 1 && !s.boff && ((uintptr_t)s.ptr % pb) == 0 && (s.dist_b % 2) == 0 &&
          (s.lpb.d == 1 || (s.dist_l % 2) == 0);
 }
 
@@ -456,7 +458,8 @@ static bool side_col(const Side &s) {
   const long long D = s.lpb.d > 1 ? s.dist_l : s.dist_b;
   return std::llabs(D) < std::llabs(s.stride);
 }
-static int choose_flags(int op, const KArgs &a) {
+int choose_flags(int op, const KArgs &a) {
+  if (op >= OP_RADER_FS1) return 0;  // gathers and scatters: row layout
   const bool fg = op_fg(op), tg = op_tg(op);
   const bool ic = side_col(a.in), oc = side_col(a.out);
   if (fg && tg) {
@@ -551,7 +554,7 @@ size_t Exec1D::ws_bytes(long long nl) const {
     case K_FOURSTEP: return 3 * (size_t)n * nl * c + 256;
     case K_RADER:
       if (fused) return 0;
-      return (2 * (size_t)cl + 2) * nl * c + 256 + sub->ws_bytes(nl);
+      return (2 * (size_t)n + 2 * (size_t)cl + 2) * nl * c + 1024;
     case K_BLUE:
       if (fused) return 0;
       return 2 * (size_t)m * nl * c + 256 + sub->ws_bytes(nl);
@@ -559,13 +562,14 @@ size_t Exec1D::ws_bytes(long long nl) const {
   }
 }
 
-static bool side_simple(const Side &s, long long &D) {
+bool side_simple(const Side &s, long long &D) {
+  if (s.boff) return false;
   if (s.lpb.d == 1) { D = s.dist_b; return true; }
   if (s.dist_b == (long long)s.lpb.d * s.dist_l) { D = s.dist_l; return true; }
   return false;
 }
 
-static char *align256(char *p) { return (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255); }
+char *align256(char *p) { return (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255); }
 
 #define GF_PREC_CALL(prec, fn, ...)                                                \
   (count_launch(), (prec) == F64 ? prec_f64::fn(__VA_ARGS__)                       \
@@ -645,39 +649,7 @@ int Exec1D::exec(const Side &in, const Side &out, long long nl, int cji, int cjo
         a.ic = cyclic ? 0 : (int)(n - 1);
         return launch_line(OP_RADER, *prog, a, nl, st, 0, true);
       }
-      char *w = align256((char *)ws);
-      char *A = w;
-      char *B = A + (size_t)cl * nl * c;
-      char *x0s = B + (size_t)cl * nl * c;
-      char *dc = x0s + (size_t)nl * c;
-      char *wsub = align256(dc + (size_t)nl * c);
-      EwArgs e{};
-      e.nlines = nl;
-      e.len = (int)(n - 1);
-      e.ldst = (int)cl;
-      e.perm = perm;
-      e.cj = cji;
-      e.x0s = x0s;
-      GF_CK(GF_PREC_CALL(prec, gather, A, in, e, st));
-      if (int rc = sub->exec(contig(A, cl), contig(B, cl), nl, 0, 0, 1.0, wsub, st)) return rc;
-      EwArgs e2{};
-      e2.nlines = nl;
-      e2.len = (int)cl;
-      e2.x0s = x0s;
-      e2.dc = dc;
-      GF_CK(GF_PREC_CALL(prec, spec_mul, B, spec, e2, st));
-      if (int rc = sub->exec(contig(B, cl), contig(A, cl), nl, 0, 0, 1.0, wsub, st)) return rc;
-      EwArgs e3{};
-      e3.nlines = nl;
-      e3.p = (int)n;
-      e3.len = (int)cl;
-      e3.off = cyclic ? 0 : (int)(n - 1);
-      e3.x0s = x0s;
-      e3.dc = dc;
-      e3.cj = cjo;
-      e3.scale = scale;
-      GF_CK(GF_PREC_CALL(prec, rader_scatter, out, A, iperm, e3, st));
-      return 0;
+      return rader_two_pass(in, out, nl, cji, cjo, scale, ws, st);
     }
     case K_BLUE: {
       if (fused) {
@@ -721,6 +693,111 @@ int Exec1D::exec(const Side &in, const Side &out, long long nl, int cji, int cjo
     }
   }
   return set_err(1, "bad executor kind");
+}
+
+// Rader whose convolution runs as a two-pass split cl = n1 * n2 (the conv
+// exec `sub` is K_FOURSTEP): four line-kernel passes (OpRaderFS1, OpRaderFS2,
+// OpC2CTwiddle, OpRaderFS4) over two workspace buffers.
+int Exec1D::rader_two_pass(const Side &in0, const Side &out0, long long nl, int cji, int cjo, double scale,
+                           void *ws, cudaStream_t st) const {
+  const size_t c = csize(prec);
+  char *w = align256((char *)ws);
+  Side in = in0, out = out0;
+  long long Din = 0, Dout = 0;
+  if (!(in.boff && in.lpb.d == 1) && !side_simple(in, Din)) {
+    EwArgs e{};
+    e.nlines = nl;
+    e.len = (int)n;
+    e.ldst = (int)n;
+    GF_CK(GF_PREC_CALL(prec, gather, w, in, e, st));
+    in = contig(w, n);
+    Din = n;
+    w += (size_t)n * nl * c;
+  }
+  char *outbuf = nullptr;
+  if (!(out.boff && out.lpb.d == 1) && !side_simple(out, Dout)) {
+    outbuf = w;
+    w += (size_t)n * nl * c;
+  }
+  char *W1 = align256(w);
+  char *W2 = W1 + (size_t)cl * nl * c;
+  char *x0s = W2 + (size_t)cl * nl * c;
+  char *dc = x0s + (size_t)nl * c;
+  std::vector<RaderPhase> ph;
+  rader_phases(in, Din, outbuf ? contig(outbuf, n) : out, outbuf ? n : Dout, nl, cji, cjo, scale, W1, W2, x0s,
+               dc, ph);
+  for (auto &q : ph)
+    if (int rc = launch_line(q.op, *q.prog, q.a, q.nlines, st)) return rc;
+  if (outbuf) {
+    EwArgs e{};
+    e.nlines = nl;
+    e.len = (int)n;
+    e.scale = 1.0;
+    GF_CK(GF_PREC_CALL(prec, scatter, out, outbuf, e, st));
+  }
+  return 0;
+}
+
+// The four passes of rader_two_pass for signals addressed by `in` / `out`
+// (signal s at s*D or boff[s], element stride), over workspaces W1, W2
+// (cl per signal) and x0s, dc (one complex per signal).
+void Exec1D::rader_phases(const Side &in, long long Din, const Side &out, long long Dout, long long nl, int cji,
+                          int cjo, double scale, void *W1, void *W2, void *x0s, void *dc,
+                          std::vector<RaderPhase> &ph) const {
+  const Exec1D &cv = *sub;
+  const long long N1 = cv.n1, N2 = cv.n2;
+  const long long q = n - 1;
+  auto sig_side = [&](const Side &s, long long D, long long lpb) {
+    Side r = mk_side(s.ptr, D, 0, s.stride, lpb);
+    r.boff = s.boff;
+    return r;
+  };
+  RaderPhase f1{};
+  f1.op = OP_RADER_FS1;
+  f1.prog = cv.p1;
+  f1.nlines = nl * N2;
+  f1.a.in = sig_side(in, Din, N2);
+  f1.a.out = mk_side(W1, cl, 1, N2, N2);
+  f1.a.cj_in = cji;
+  f1.a.scale = 1.0;
+  f1.a.aux0 = perm;
+  f1.a.aux1 = cv.tw4;
+  f1.a.aux2 = x0s;
+  f1.a.ia = cl;
+  f1.a.ib = q;
+  RaderPhase f2{};
+  f2.op = OP_RADER_FS2;
+  f2.prog = cv.p2;
+  f2.nlines = nl * N1;
+  f2.a.in = mk_side(W1, cl, N2, 1, N1);
+  f2.a.out = mk_side(W2, cl, 1, N1, N1);
+  f2.a.scale = 1.0;
+  f2.a.aux0 = spec;
+  f2.a.aux1 = x0s;
+  f2.a.aux2 = dc;
+  RaderPhase f3{};
+  f3.op = OP_C2C_TW;
+  f3.prog = cv.p1;
+  f3.nlines = nl * N2;
+  f3.a.in = mk_side(W2, cl, 1, N2, N2);
+  f3.a.out = mk_side(W1, cl, 1, N2, N2);
+  f3.a.scale = 1.0;
+  f3.a.aux0 = cv.tw4;
+  f3.a.ia = cl;
+  RaderPhase f4{};
+  f4.op = OP_RADER_FS4;
+  f4.prog = cv.p2;
+  f4.nlines = nl * N1;
+  f4.a.in = mk_side(W1, cl, N2, 1, N1);
+  f4.a.out = sig_side(out, Dout, N1);
+  f4.a.cj_out = cjo;
+  f4.a.scale = scale;
+  f4.a.aux0 = iperm;
+  f4.a.aux1 = x0s;
+  f4.a.aux2 = dc;
+  f4.a.ia = q;
+  f4.a.ib = cyclic ? 0 : q;
+  ph = {f1, f2, f3, f4};
 }
 
 std::string Exec1D::describe() const {

@@ -52,6 +52,15 @@ struct DevProg {
 
 enum ExecKind { K_SINGLE = 0, K_FOURSTEP = 1, K_RADER = 2, K_BLUE = 3 };
 
+struct DevProg;
+// One line-kernel pass of a multi-pass transform.
+struct RaderPhase {
+  int op;
+  std::shared_ptr<DevProg> prog;
+  KArgs a;
+  long long nlines;
+};
+
 struct Exec1D {
   long long n = 0;
   int prec = 0, kind = K_SINGLE, device = 0;
@@ -70,6 +79,11 @@ struct Exec1D {
   size_t ws_bytes(long long nlines) const;
   int exec(const Side &in, const Side &out, long long nlines, int cj_in, int cj_out, double scale,
            void *ws, cudaStream_t st) const;
+  int rader_two_pass(const Side &in, const Side &out, long long nlines, int cj_in, int cj_out, double scale,
+                     void *ws, cudaStream_t st) const;
+  void rader_phases(const Side &in, long long Din, const Side &out, long long Dout, long long nl, int cji,
+                    int cjo, double scale, void *W1, void *W2, void *x0s, void *dc,
+                    std::vector<RaderPhase> &ph) const;
   std::string describe() const;
 };
 
@@ -99,6 +113,11 @@ std::shared_ptr<const ExecReal> get_real(long long n, int prec);
 bool fits_single(long long n, int prec);
 bool pairs_aligned(const Side &s, int prec);
 
+bool side_simple(const Side &s, long long &D);
+char *align256(char *p);
+int choose_lpc(const DevProg &dp, const KArgs &a, int op, long long nlines, bool conv);
+int choose_flags(int op, const KArgs &a);
+
 // Launch helper for the line kernels.
 int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st,
                 int lpc = 0, bool conv = false);
@@ -110,6 +129,7 @@ inline Side mk_side(void *p, long long dist_b, long long dist_l, long long strid
   s.dist_l = dist_l;
   s.stride = stride;
   s.lpb = FastDiv((uint32_t)(lpb < 1 ? 1 : lpb));
+  s.boff = nullptr;
   return s;
 }
 // Contiguous lines of length len.

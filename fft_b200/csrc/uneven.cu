@@ -1,0 +1,438 @@
+// uneven.cu -- many 1-D complex transforms of different lengths in one
+// persistent launch.
+//
+// The signals are grouped by length.  Each length's executor is lowered to a
+// list of phases (one line op over a number of tiles): one phase for a length
+// that fits one CTA (and for a Rader or Bluestein transform whose convolution
+// fits one CTA), two for the four-step split, four for Rader over a two-pass
+// convolution.  Phases are ordered by dependency level (every first phase,
+// then every second phase, ...) and executed by k_persist, whose CTAs claim
+// (phase, tile) items from a counter; a phase waits, with a bounded spin, for
+// the phase it depends on.  The same phases can also be launched one kernel
+// each (the non-persistent mode, used to check the scheduler).
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <sstream>
+
+#include "../../include/gofft.h"
+#include "kernels.cuh"
+#include "plan.cuh"
+
+using namespace gf;
+
+#define GF_CK(x)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess)                                                              \
+      return set_err(GOFFT_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+namespace {
+// Placeholders for the caller's packed input / output, patched per call.
+char g_in_tag, g_out_tag;
+}  // namespace
+
+struct gofft_uneven {
+  int prec = 0, device = 0, persistent = 1;
+  long long count = 0;
+  struct Cls {
+    long long n = 0;
+    std::vector<long long> sig;
+    std::shared_ptr<const Exec1D> ex;
+    long long *d_ioff = nullptr, *d_ooff = nullptr;
+  };
+  std::vector<Cls> cls;
+  std::vector<PhaseDesc> ph[2];        // forward, inverse (user pointers as tags)
+  std::vector<int> ph_level;
+  std::vector<std::shared_ptr<DevProg>> ph_prog;
+  PhaseDesc *d_ph[2] = {nullptr, nullptr};
+  PhaseDesc *h_pinned = nullptr;       // staging for pointer patches
+  void *ws = nullptr;
+  size_t ws_bytes = 0;
+  unsigned long long *d_ctr = nullptr;  // counter, then done[nph], err
+  int nph = 0, block = 0;
+  long long total = 0;
+  size_t smem = 0;
+  int grid = 0;
+  long long spin_limit = 1ll << 24;
+  int extra_wait = 0;                  // test hook: a dependency that never completes
+  const void *last_in[2] = {nullptr, nullptr};
+  void *last_out[2] = {nullptr, nullptr};
+  ~gofft_uneven() {
+    for (auto &c : cls) {
+      if (c.d_ioff) cudaFree(c.d_ioff);
+      if (c.d_ooff) cudaFree(c.d_ooff);
+    }
+    for (auto p : d_ph)
+      if (p) cudaFree(p);
+    if (h_pinned) cudaFreeHost(h_pinned);
+    if (ws) cudaFree(ws);
+    if (d_ctr) cudaFree(d_ctr);
+  }
+};
+
+static int *done_ptr(gofft_uneven *u) { return reinterpret_cast<int *>(u->d_ctr + 1); }
+static int *err_ptr(gofft_uneven *u) { return done_ptr(u) + u->nph; }
+
+static Side tag_side(char *tag, const long long *boff, long long dist_l, long long stride, long long lpb) {
+  Side s = mk_side(tag, 0, dist_l, stride, lpb);
+  s.boff = boff;
+  return s;
+}
+
+// Appends the phases of one length class.  Sides on the caller's buffers
+// carry the tags; workspace regions are carved from *wsoff.
+static int add_class(gofft_uneven *u, gofft_uneven::Cls &c, size_t *wsoff, std::vector<PhaseDesc> &out,
+                     std::vector<int> &level, std::vector<std::shared_ptr<DevProg>> &progs) {
+  const Exec1D &e = *c.ex;
+  const long long cnt = (long long)c.sig.size();
+  const size_t cs = csize(u->prec);
+  auto carve = [&](size_t bytes) {
+    const size_t off = (*wsoff + 255) & ~(size_t)255;
+    *wsoff = off + bytes;
+    return (char *)nullptr + off;  // offset; rebased once the workspace exists
+  };
+  auto push = [&](int op, const std::shared_ptr<DevProg> &prog, KArgs a, long long nlines, int dep, int lvl,
+                  bool conv) {
+    PhaseDesc p{};
+    a.lp = prog->lp;
+    a.nlines = nlines;
+    a.lpc = choose_lpc(*prog, a, op, nlines, conv);
+    a.ndiv = FastDiv((uint32_t)prog->n);
+    a.lpcdiv = FastDiv((uint32_t)a.lpc);
+    a.flags = choose_flags(op, a) & GF_COLMAP;
+    p.a = a;
+    p.op = op;
+    p.dep = dep;
+    p.ntiles = (nlines + a.lpc - 1) / a.lpc;
+    out.push_back(p);
+    level.push_back(lvl);
+    progs.push_back(prog);
+    return (int)out.size() - 1;
+  };
+  const Side in1 = tag_side(&g_in_tag, c.d_ioff, 0, 1, 1);
+  const Side out1 = tag_side(&g_out_tag, c.d_ooff, 0, 1, 1);
+  if (e.kind == K_SINGLE) {
+    KArgs a{};
+    a.in = in1;
+    a.out = out1;
+    a.scale = 1.0;
+    push(OP_C2C, e.prog, a, cnt, -1, 0, false);
+    return 0;
+  }
+  if (e.kind == K_FOURSTEP) {
+    char *w = carve((size_t)e.n * cnt * cs);
+    KArgs a1{};
+    a1.in = tag_side(&g_in_tag, c.d_ioff, 1, e.n2, e.n2);
+    a1.out = mk_side(w, e.n, 1, e.n2, e.n2);
+    a1.scale = 1.0;
+    a1.aux0 = e.tw4;
+    a1.ia = e.n;
+    const int p1 = push(OP_C2C_TW, e.p1, a1, cnt * e.n2, -1, 0, false);
+    KArgs a2{};
+    a2.in = mk_side(w, e.n, e.n2, 1, e.n1);
+    a2.out = tag_side(&g_out_tag, c.d_ooff, 1, e.n1, e.n1);
+    a2.scale = 1.0;
+    push(OP_C2C, e.p2, a2, cnt * e.n1, p1, 1, false);
+    return 0;
+  }
+  if (e.kind == K_RADER && e.fused) {
+    KArgs a{};
+    a.in = in1;
+    a.out = out1;
+    a.scale = 1.0;
+    a.aux0 = e.perm;
+    a.aux1 = e.iperm;
+    a.aux2 = e.spec;
+    a.ia = e.n;
+    a.ic = e.cyclic ? 0 : (int)(e.n - 1);
+    push(OP_RADER, e.prog, a, cnt, -1, 0, true);
+    return 0;
+  }
+  if (e.kind == K_BLUE && e.fused) {
+    KArgs a{};
+    a.in = in1;
+    a.out = out1;
+    a.scale = 1.0;
+    a.aux0 = e.chirp;
+    a.aux2 = e.spec;
+    a.ia = e.n;
+    push(OP_BLUE, e.prog, a, cnt, -1, 0, true);
+    return 0;
+  }
+  if (e.kind == K_RADER && e.sub && e.sub->kind == K_FOURSTEP) {
+    char *W1 = carve((size_t)e.cl * cnt * cs);
+    char *W2 = carve((size_t)e.cl * cnt * cs);
+    char *x0s = carve((size_t)cnt * cs);
+    char *dc = carve((size_t)cnt * cs);
+    std::vector<RaderPhase> rp;
+    e.rader_phases(in1, 0, out1, 0, cnt, 0, 0, 1.0, W1, W2, x0s, dc, rp);
+    int prev = -1;
+    for (size_t i = 0; i < rp.size(); i++) prev = push(rp[i].op, rp[i].prog, rp[i].a, rp[i].nlines, prev, (int)i, false);
+    return 0;
+  }
+  return set_err(GOFFT_EUNSUPPORTED, "length " + std::to_string(c.n) + " has no persistent schedule");
+}
+
+// Replaces the tags and workspace offsets of one side.
+static void rebase_side(Side &s, char *ws, const void *in, void *out) {
+  if (s.ptr == &g_in_tag) s.ptr = (void *)in;
+  else if (s.ptr == &g_out_tag) s.ptr = out;
+  else if ((uintptr_t)s.ptr < ((uintptr_t)1 << 40) && ws) s.ptr = ws + (uintptr_t)s.ptr;
+}
+static void rebase_aux(const void *&p, char *ws, size_t wsb) {
+  if ((uintptr_t)p < wsb + 256 && p != nullptr) p = ws + (uintptr_t)p;
+}
+
+extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_t count, const int64_t *in_offsets,
+                                   const int64_t *out_offsets, gofft_uneven **out) {
+  if (!out || !lengths || count <= 0) return set_err(GOFFT_EINVAL, "bad uneven batch arguments");
+  *out = nullptr;
+  if (precision < 0 || precision > 2) return set_err(GOFFT_EINVAL, "bad precision");
+  std::unique_ptr<gofft_uneven> u(new gofft_uneven());
+  u->prec = precision;
+  u->count = count;
+  cudaGetDevice(&u->device);
+  std::vector<long long> ioff(count), ooff(count);
+  long long acc = 0;
+  for (int64_t i = 0; i < count; i++) {
+    if (lengths[i] < 1) return set_err(GOFFT_EINVAL, "uneven batch lengths must be positive");
+    ioff[i] = in_offsets ? in_offsets[i] : acc;
+    ooff[i] = out_offsets ? out_offsets[i] : ioff[i];
+    acc += lengths[i];
+  }
+  std::map<long long, size_t> byn;
+  for (int64_t i = 0; i < count; i++) {
+    auto it = byn.find(lengths[i]);
+    if (it == byn.end()) {
+      byn[lengths[i]] = u->cls.size();
+      u->cls.emplace_back();
+      u->cls.back().n = lengths[i];
+      it = byn.find(lengths[i]);
+    }
+    u->cls[it->second].sig.push_back(i);
+  }
+  // per-class offset tables and executors
+  for (auto &c : u->cls) {
+    c.ex = get_exec(c.n, precision);
+    if (!c.ex) return GOFFT_ECUDA;
+    std::vector<long long> a, b;
+    for (long long s : c.sig) {
+      a.push_back(ioff[s]);
+      b.push_back(ooff[s]);
+    }
+    GF_CK(cudaMalloc(&c.d_ioff, a.size() * sizeof(long long)));
+    GF_CK(cudaMalloc(&c.d_ooff, b.size() * sizeof(long long)));
+    GF_CK(cudaMemcpy(c.d_ioff, a.data(), a.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    GF_CK(cudaMemcpy(c.d_ooff, b.data(), b.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  }
+  // phases (forward), in per-class order first
+  std::vector<PhaseDesc> raw;
+  std::vector<int> lvl;
+  std::vector<std::shared_ptr<DevProg>> progs;
+  size_t wsoff = 0;
+  for (auto &c : u->cls)
+    if (int rc = add_class(u.get(), c, &wsoff, raw, lvl, progs)) return rc;
+  // order by level, keeping class order within a level; remap dependencies
+  std::vector<int> order(raw.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return lvl[x] < lvl[y]; });
+  std::vector<int> pos(raw.size());
+  for (size_t i = 0; i < order.size(); i++) pos[order[i]] = (int)i;
+  u->nph = (int)raw.size();
+  u->ph[0].resize(u->nph);
+  long long first = 0;
+  for (int i = 0; i < u->nph; i++) {
+    PhaseDesc p = raw[order[i]];
+    if (p.dep >= 0) p.dep = pos[p.dep];
+    p.first = first;
+    first += p.ntiles;
+    u->ph[0][i] = p;
+    u->ph_level.push_back(lvl[order[i]]);
+    u->ph_prog.push_back(progs[order[i]]);
+  }
+  u->total = first;
+  // workspace and counters
+  u->ws_bytes = wsoff;
+  if (wsoff) GF_CK(cudaMalloc(&u->ws, wsoff));
+  for (auto &p : u->ph[0]) {
+    rebase_side(p.a.in, (char *)u->ws, &g_in_tag, &g_out_tag);
+    rebase_side(p.a.out, (char *)u->ws, &g_in_tag, &g_out_tag);
+    rebase_aux(p.a.aux0, (char *)u->ws, u->ws_bytes);
+    rebase_aux(p.a.aux1, (char *)u->ws, u->ws_bytes);
+    rebase_aux(p.a.aux2, (char *)u->ws, u->ws_bytes);
+  }
+  // inverse table: conjugate in on each level-0 phase, out on each last phase
+  u->ph[1] = u->ph[0];
+  for (int i = 0; i < u->nph; i++) {
+    bool has_child = false;
+    for (int j = 0; j < u->nph; j++)
+      if (u->ph[0][j].dep == i) has_child = true;
+    PhaseDesc &p = u->ph[1][i];
+    if (p.dep < 0) p.a.cj_in = 1;
+    if (!has_child) {
+      p.a.cj_out = 1;
+      p.a.scale = 1.0;  // set below per class length
+    }
+  }
+  // scale 1/n on the last phase of each class: find the class length by walking
+  // the class order (phases of a class share the executor length)
+  {
+    size_t k = 0;
+    std::vector<long long> len_of(raw.size());
+    for (auto &c : u->cls) {
+      const Exec1D &e = *c.ex;
+      int np = e.kind == K_FOURSTEP ? 2 : (e.kind == K_RADER && !e.fused ? 4 : 1);
+      for (int t = 0; t < np; t++) len_of[k++] = c.n;
+    }
+    for (int i = 0; i < u->nph; i++) {
+      bool has_child = false;
+      for (int j = 0; j < u->nph; j++)
+        if (u->ph[1][j].dep == i) has_child = true;
+      if (!has_child) u->ph[1][i].a.scale = 1.0 / (double)len_of[order[i]];
+    }
+  }
+  // launch shape: enough threads and shared memory for every phase
+  for (int i = 0; i < u->nph; i++) {
+    const PhaseDesc &p = u->ph[0][i];
+    const bool conv = p.op == OP_RADER || p.op == OP_BLUE;
+    u->block = std::max(u->block, p.a.lpc * p.a.lp.T);
+    u->smem = std::max(u->smem, (size_t)p.a.lpc * spad_size(p.a.lp.n) * csize(precision) +
+                                    (conv ? 2 * p.a.lpc * csize(precision) : 0));
+  }
+  u->block = (u->block + 31) / 32 * 32;
+  const void *kp = precision == F64 ? (const void *)k_persist<PrecF64>
+                   : precision == F32 ? (const void *)k_persist<PrecF32>
+                                      : (const void *)k_persist<PrecF32C>;
+  if (u->smem > 48 * 1024) GF_CK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u->smem));
+  int per_sm = 0, sms = 0;
+  GF_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kp, u->block, u->smem));
+  GF_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, u->device));
+  if (per_sm < 1) return set_err(GOFFT_EUNSUPPORTED, "persistent kernel does not fit an SM");
+  u->grid = (int)std::min<long long>((long long)per_sm * sms, u->total);
+  for (int d = 0; d < 2; d++) GF_CK(cudaMalloc(&u->d_ph[d], u->nph * sizeof(PhaseDesc)));
+  GF_CK(cudaMallocHost(&u->h_pinned, u->nph * sizeof(PhaseDesc)));
+  GF_CK(cudaMalloc(&u->d_ctr, sizeof(unsigned long long) * (2 + (u->nph + 2) / 2)));
+  *out = u.release();
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_uneven_destroy(gofft_uneven *u) {
+  delete u;
+  return GOFFT_OK;
+}
+
+// Writes the phase table for (in, out) when the buffers differ from the last
+// call in this direction (not allowed while the stream is being captured).
+static int patch(gofft_uneven *u, int dir, const void *in, void *out, cudaStream_t st) {
+  if (u->last_in[dir] == in && u->last_out[dir] == out) return 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(st, &cs);
+  if (cs != cudaStreamCaptureStatusNone)
+    return set_err(GOFFT_EINVAL, "run the uneven batch once on these buffers before capturing it");
+  std::vector<PhaseDesc> t = u->ph[dir];
+  for (auto &p : t) {
+    if (p.a.in.ptr == &g_in_tag) p.a.in.ptr = (void *)in;
+    if (p.a.in.ptr == &g_out_tag) p.a.in.ptr = out;
+    if (p.a.out.ptr == &g_out_tag) p.a.out.ptr = out;
+    if (p.a.out.ptr == &g_in_tag) p.a.out.ptr = (void *)in;
+  }
+  if (u->extra_wait && u->nph > 1) {
+    // test hook: make the last phase wait on a phase that never completes
+    t[u->nph - 1].dep = 0;
+    t[0].ntiles += 1;
+  }
+  GF_CK(cudaStreamSynchronize(st));
+  GF_CK(cudaMemcpy(u->d_ph[dir], t.data(), u->nph * sizeof(PhaseDesc), cudaMemcpyHostToDevice));
+  u->last_in[dir] = in;
+  u->last_out[dir] = out;
+  return 0;
+}
+
+extern "C" int gofft_uneven_exec(gofft_uneven *u, const void *in, void *out, int inverse, gofft_stream stream) {
+  if (!u || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int dir = inverse ? 1 : 0;
+  if (int rc = patch(u, dir, in, out, st)) return rc;
+  if (u->persistent) {
+    GF_CK(cudaMemsetAsync(u->d_ctr, 0, sizeof(unsigned long long) * (2 + (u->nph + 2) / 2), st));
+    count_launch();
+    switch (u->prec) {
+      case F64:
+        k_persist<PrecF64><<<u->grid, u->block, u->smem, st>>>(u->d_ph[dir], u->nph, u->total, u->d_ctr,
+                                                                done_ptr(u), err_ptr(u), u->spin_limit);
+        break;
+      case F32:
+        k_persist<PrecF32><<<u->grid, u->block, u->smem, st>>>(u->d_ph[dir], u->nph, u->total, u->d_ctr,
+                                                                done_ptr(u), err_ptr(u), u->spin_limit);
+        break;
+      default:
+        k_persist<PrecF32C><<<u->grid, u->block, u->smem, st>>>(u->d_ph[dir], u->nph, u->total, u->d_ctr,
+                                                                 done_ptr(u), err_ptr(u), u->spin_limit);
+        break;
+    }
+    GF_CK(cudaGetLastError());
+    return GOFFT_OK;
+  }
+  // one launch per phase, in phase order (dependencies are earlier phases)
+  std::vector<PhaseDesc> t = u->ph[dir];
+  for (int i = 0; i < u->nph; i++) {
+    PhaseDesc p = t[i];
+    if (p.a.in.ptr == &g_in_tag) p.a.in.ptr = (void *)in;
+    if (p.a.out.ptr == &g_out_tag) p.a.out.ptr = out;
+    const bool conv = p.op == OP_RADER || p.op == OP_BLUE;
+    if (int rc = launch_line(p.op, *u->ph_prog[i], p.a, p.a.nlines, st, p.a.lpc, conv)) return rc;
+  }
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_uneven_status(gofft_uneven *u) {
+  if (!u) return set_err(GOFFT_EINVAL, "null argument");
+  int err = 0;
+  GF_CK(cudaDeviceSynchronize());
+  GF_CK(cudaMemcpy(&err, err_ptr(u), sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) return set_err(GOFFT_ETIMEOUT, "a persistent-kernel wait timed out");
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_uneven_set(gofft_uneven *u, int what, int64_t value) {
+  if (!u) return set_err(GOFFT_EINVAL, "null argument");
+  switch (what) {
+    case 0: u->persistent = value ? 1 : 0; break;
+    case 1: u->spin_limit = value > 0 ? value : 1; break;
+    case 2:
+      u->extra_wait = value ? 1 : 0;
+      u->last_in[0] = u->last_in[1] = nullptr;
+      u->last_out[0] = u->last_out[1] = nullptr;
+      break;
+    default: return set_err(GOFFT_EINVAL, "bad setting");
+  }
+  return GOFFT_OK;
+}
+
+extern "C" int64_t gofft_uneven_describe(const gofft_uneven *u, char *buf, int64_t cap) {
+  if (!u) return -1;
+  std::ostringstream o;
+  o << "{\"count\":" << u->count << ",\"precision\":" << u->prec << ",\"phases\":" << u->nph
+    << ",\"items\":" << u->total << ",\"grid\":" << u->grid << ",\"block\":" << u->block << ",\"smem\":" << u->smem
+    << ",\"workspace\":" << u->ws_bytes << ",\"classes\":[";
+  for (size_t i = 0; i < u->cls.size(); i++)
+    o << (i ? "," : "") << "{\"n\":" << u->cls[i].n << ",\"count\":" << u->cls[i].sig.size()
+      << ",\"exec\":" << u->cls[i].ex->describe() << "}";
+  o << "],\"phase_list\":[";
+  for (int i = 0; i < u->nph; i++) {
+    const PhaseDesc &p = u->ph[0][i];
+    o << (i ? "," : "") << "{\"op\":" << p.op << ",\"n\":" << p.a.lp.n << ",\"lines\":" << p.a.nlines
+      << ",\"lpc\":" << p.a.lpc << ",\"tiles\":" << p.ntiles << ",\"dep\":" << p.dep
+      << ",\"level\":" << u->ph_level[i] << "}";
+  }
+  o << "]}";
+  const std::string s = o.str();
+  if (buf && cap > 0) {
+    const size_t k = std::min<size_t>(s.size(), (size_t)cap - 1);
+    memcpy(buf, s.data(), k);
+    buf[k] = 0;
+  }
+  return (int64_t)s.size();
+}

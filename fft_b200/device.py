@@ -143,3 +143,81 @@ def spectrogram(x, segment, overlap, window, d, precision="f64", stream=None):
                                              ctypes.c_void_p(out.data_ptr()), ctypes.byref(nf),
                                              _stream(stream)))
     return out
+
+
+class UnevenBatch:
+    """Complex transforms of different lengths in one persistent launch
+    (gofft_uneven_*).  Signals are packed back to back in one tensor unless
+    offsets are given."""
+
+    def __init__(self, precision, lengths, in_offsets=None, out_offsets=None):
+        self.prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        self.lengths = [int(n) for n in lengths]
+        n = len(self.lengths)
+        L = (ctypes.c_int64 * n)(*self.lengths)
+        io = (ctypes.c_int64 * n)(*in_offsets) if in_offsets is not None else None
+        oo = (ctypes.c_int64 * n)(*out_offsets) if out_offsets is not None else None
+        h = ctypes.c_void_p()
+        check(lib().gofft_uneven_create(self.prec, L, n, io, oo, ctypes.byref(h)))
+        self._h = h
+        self.cdtype = CDT[self.prec]
+
+    def __call__(self, x, out=None, inverse=False, stream=None):
+        _need(x, self.cdtype, "x")
+        if out is None:
+            out = torch.empty_like(x)
+        check(lib().gofft_uneven_exec(self._h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                      1 if inverse else 0, _stream(stream)))
+        return out
+
+    def status(self):
+        return lib().gofft_uneven_status(self._h)
+
+    def set(self, what, value):
+        check(lib().gofft_uneven_set(self._h, int(what), int(value)))
+
+    def describe(self):
+        n = lib().gofft_uneven_describe(self._h, None, 0)
+        buf = ctypes.create_string_buffer(int(n) + 1)
+        lib().gofft_uneven_describe(self._h, buf, n + 1)
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if self._h:
+            lib().gofft_uneven_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    """A captured sequence of engine calls on a (non-default) stream."""
+
+    def __init__(self, stream):
+        self.stream = stream
+        self._h = None
+
+    def __enter__(self):
+        check(lib().gofft_graph_begin(ctypes.c_void_p(self.stream.cuda_stream)))
+        return self
+
+    def __exit__(self, *exc):
+        h = ctypes.c_void_p()
+        st = lib().gofft_graph_end(ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(h))
+        if exc[0] is None:
+            check(st)
+        self._h = h
+
+    def replay(self):
+        check(lib().gofft_graph_launch(self._h, ctypes.c_void_p(self.stream.cuda_stream)))
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().gofft_graph_destroy(self._h)
+        except Exception:
+            pass

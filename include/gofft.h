@@ -177,6 +177,44 @@ GOFFT_API int gofft_spectrogram_device(int precision, const void *x, int64_t nx,
                              int64_t *nframes, gofft_stream stream);
 
 /* ------------------------------------------------------------------------ */
+/* 2b. Uneven batches (no counterpart in the reference, whose batches are a   */
+/*     caller loop over Plan.FFT, plan.go:91): many complex transforms of     */
+/*     different lengths in one persistent launch.                            */
+/* ------------------------------------------------------------------------ */
+typedef struct gofft_uneven gofft_uneven;
+/* count signals; signal i has lengths[i] elements at in_offsets[i] of the
+ * packed input and out_offsets[i] of the packed output (elements of the
+ * precision's complex type; NULL offsets = packed back to back, out = in). */
+GOFFT_API int gofft_uneven_create(int precision, const int64_t *lengths, int64_t count,
+                                  const int64_t *in_offsets, const int64_t *out_offsets,
+                                  gofft_uneven **out);
+GOFFT_API int gofft_uneven_destroy(gofft_uneven *u);
+/* Forward or normalised inverse of every signal: one persistent kernel (plus a
+ * counter reset) on `stream`; capturable in a CUDA graph once the batch has
+ * run on the same buffers.  Errors of the device-side waits are reported by
+ * gofft_uneven_status. */
+GOFFT_API int gofft_uneven_exec(gofft_uneven *u, const void *in, void *out, int inverse,
+                                gofft_stream stream);
+/* Synchronises and returns GOFFT_ETIMEOUT if a bounded wait of the last run
+ * expired (its results are then invalid). */
+GOFFT_API int gofft_uneven_status(gofft_uneven *u);
+/* what = 0: persistent (1, default) or one launch per phase (0);
+ * 1: poll limit of the device-side waits; 2: test hook that makes one wait
+ * depend on work that never completes (to exercise the timeout path). */
+GOFFT_API int gofft_uneven_set(gofft_uneven *u, int what, int64_t value);
+GOFFT_API int64_t gofft_uneven_describe(const gofft_uneven *u, char *buf, int64_t cap);
+
+/* ------------------------------------------------------------------------ */
+/* 2c. CUDA graphs: capture any sequence of gofft_exec_* / gofft_uneven_exec */
+/*     calls on a stream and replay it.                                      */
+/* ------------------------------------------------------------------------ */
+typedef struct gofft_graph gofft_graph;
+GOFFT_API int gofft_graph_begin(gofft_stream stream);
+GOFFT_API int gofft_graph_end(gofft_stream stream, gofft_graph **out);
+GOFFT_API int gofft_graph_launch(gofft_graph *g, gofft_stream stream);
+GOFFT_API int gofft_graph_destroy(gofft_graph *g);
+
+/* ------------------------------------------------------------------------ */
 /* 3. Instrumentation and tuning (no counterpart in the reference).          */
 /* ------------------------------------------------------------------------ */
 
