@@ -779,3 +779,63 @@ extern "C" int gofft_graph_destroy(gofft_graph *g) {
   delete g;
   return GOFFT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Complex transform that allocates nothing.
+//
+// gofft_exec_c2c() runs multi-pass transforms (lengths split into two passes,
+// and primes whose convolution is split) through the plan's own workspace.
+// Some callers cannot have any device memory allocated on their behalf while
+// they run: code that records work into a CUDA graph (allocation calls are not
+// part of the captured stream and can invalidate the capture), programs whose
+// device memory is owned and budgeted by another allocator's pool, and paths
+// where the device-wide synchronisation of cudaMalloc/cudaFree is not
+// acceptable.  For them this entry point takes its scratch from one
+// fixed-size array that is part of the library image: it never calls
+// cudaMalloc, cudaFree or any allocating routine.
+//
+// The array, kNoAllocScratchBytes (16 MiB), is held by every GPU that loads
+// the library until the process exits.  Host code cannot use the symbol's
+// address directly (it names a host-side stand-in), so the device address is
+// looked up once per device with cudaGetSymbolAddress, by the first call on
+// that device; make that first call before starting any stream capture.
+// Every call uses the same array and it keeps whatever the last call left:
+// nothing in it needs to start at zero (each pass writes all the scratch it
+// later reads), but calls whose executions overlap on the GPU (different
+// streams, or different threads) race on it and must be serialised by the
+// caller.
+// ---------------------------------------------------------------------------
+static constexpr size_t kNoAllocScratchBytes = 16u << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static std::map<int, void *> g_noalloc_addr;
+
+extern "C" int gofft_exec_c2c_noalloc(gofft_plan *p, const void *in, void *out, int inverse,
+                                      gofft_stream stream) {
+  if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_C2C || p->rank != 1)
+    return set_err(GOFFT_EUNSUPPORTED, "the no-allocation entry point takes 1-D complex plans");
+  const size_t need = p->ax[0]->ws_bytes(p->batch);
+  if (need > kNoAllocScratchBytes)
+    return set_err(GOFFT_EINVAL, "transform needs " + std::to_string(need) +
+                                     " bytes of scratch; the no-allocation entry point has " +
+                                     std::to_string(kNoAllocScratchBytes));
+  int dev = 0;
+  GF_CK(cudaGetDevice(&dev));
+  void *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    auto it = g_noalloc_addr.find(dev);
+    if (it == g_noalloc_addr.end()) {
+      void *ptr = nullptr;
+      GF_CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+      it = g_noalloc_addr.emplace(dev, ptr).first;
+    }
+    scratch = it->second;
+  }
+  const int cj = inverse ? 1 : 0;
+  const double sc = inverse ? 1.0 / (double)p->shape[0] : 1.0;
+  return p->ax[0]->exec(mk_side((void *)in, p->idist, 0, p->istride, 1), mk_side(out, p->odist, 0, p->ostride, 1),
+                        p->batch, cj, cj, sc, need ? scratch : nullptr, (cudaStream_t)stream);
+}

@@ -155,6 +155,19 @@ GOFFT_API int gofft_exec_r2c(gofft_plan *p, const void *in, void *out, gofft_str
  * (nbins <= 0 means n/2+1); output normalised by 1/prod(shape). */
 GOFFT_API int gofft_exec_c2r(gofft_plan *p, const void *in, int64_t nbins, void *out, gofft_stream stream);
 
+/* gofft_exec_c2c for a 1-D complex plan without allocating anything (no
+ * counterpart in the reference, whose transforms allocate per call).  For
+ * callers that cannot have device memory allocated while they run -- work
+ * being recorded into a CUDA graph, device memory owned by another allocator's
+ * budget, or paths that cannot afford cudaMalloc's device-wide
+ * synchronisation.  Scratch comes from one 16 MiB array built into the
+ * library (held on every GPU that loads it); transforms needing more return
+ * GOFFT_EINVAL.  The first call on a device looks the array up and should come
+ * before any stream capture.  All calls share the array: calls whose
+ * executions overlap on the GPU race and must be serialised by the caller. */
+GOFFT_API int gofft_exec_c2c_noalloc(gofft_plan *p, const void *in, void *out, int inverse,
+                                     gofft_stream stream);
+
 /* Host-pointer variants: copy host -> device, execute, copy back, synchronise.
  * Pinned host memory makes the copies asynchronous DMA. */
 GOFFT_API int gofft_exec_c2c_host(gofft_plan *p, const void *in, void *out, int inverse);
