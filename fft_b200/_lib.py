@@ -56,6 +56,11 @@ SIGNATURES = {
     "gofft_exec_r2c": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "gofft_exec_c2r": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "gofft_exec_c2c_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
+    "gofft_vjp_c2c": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
+    "gofft_vjp_r2c": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "gofft_vjp_c2r": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "gofft_filter2_forward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "gofft_vjp_filter2": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gofft_exec_c2c_host": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
     "gofft_exec_r2c_host": (ctypes.c_int, [_vp, _vp, _vp]),
     "gofft_exec_c2r_host": (ctypes.c_int, [_vp, _vp, _i64, _vp]),

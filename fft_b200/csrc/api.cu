@@ -205,10 +205,12 @@ extern "C" int64_t gofft_plan_table(const gofft_plan *p, int which, int64_t *out
 // ---------------------------------------------------------------------------
 // Execution on device pointers
 // ---------------------------------------------------------------------------
-static int exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, cudaStream_t st) {
-  const int cj = inverse ? 1 : 0;
+// cj: transform direction (1 = inverse, as conj(FFT(conj .))); scaled: apply
+// the inverse's 1/n per axis.  The plain transforms have cj == scaled; the
+// adjoints flip the direction and keep the scaling.
+static int exec_c2c_dir(gofft_plan *p, const void *in, void *out, int cj, int scaled, cudaStream_t st) {
   if (p->rank == 1) {
-    const double sc = inverse ? 1.0 / (double)p->shape[0] : 1.0;
+    const double sc = scaled ? 1.0 / (double)p->shape[0] : 1.0;
     return p->ax[0]->exec(mk_side((void *)in, p->idist, 0, p->istride, 1),
                           mk_side(out, p->odist, 0, p->ostride, 1), p->batch, cj, cj, sc, p->ws, st);
   }
@@ -228,7 +230,7 @@ static int exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, cudaS
       const Side sd_in = mk_side(first ? (void *)src : (void *)dst, L * inner, 1, inner, inner);
       const Side sd_out = mk_side(dst, L * inner, 1, inner, inner);
       const long long lines = per * (p->total / L);
-      const double sc = inverse ? 1.0 / (double)L : 1.0;
+      const double sc = scaled ? 1.0 / (double)L : 1.0;
       if (int rc = p->ax[a]->exec(sd_in, sd_out, lines, cj, cj, sc, p->ws, st)) return rc;
       first = false;
     }
@@ -237,10 +239,16 @@ static int exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, cudaS
   return GOFFT_OK;
 }
 
-static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st) {
+static int exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, cudaStream_t st) {
+  return exec_c2c_dir(p, in, out, inverse ? 1 : 0, inverse ? 1 : 0, st);
+}
+
+// wsc != 0: the adjoint of the inverse (edge-bin weighting with scale wsc on
+// the row pass, the only real one).
+static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st, double wsc = 0.0) {
   if (p->rank == 1) {
     return p->rx->r2c(mk_side((void *)in, p->idist, 0, p->istride, 1), mk_side(out, p->odist, 0, p->ostride, 1),
-                      p->batch, p->ws, st);
+                      p->batch, p->ws, st, wsc);
   }
   const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
   const size_t r = rsize(p->prec), c = csize(p->prec);
@@ -250,7 +258,7 @@ static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st) {
     const char *src = (const char *)in + (size_t)b0 * rows * cols * r;
     char *dst = (char *)out + (size_t)b0 * rows * rc * c;
     // rows: real transform along the last axis (rfft2.go:41-51)
-    if (int e = p->rx->r2c(contig((void *)src, cols), contig(dst, rc), nb * rows, wsx, st)) return e;
+    if (int e = p->rx->r2c(contig((void *)src, cols), contig(dst, rc), nb * rows, wsx, st, wsc)) return e;
     // columns: complex transform down each of the rc columns (rfft2.go:53-72)
     if (rows > 1) {
       const Side cs = mk_side(dst, rows * rc, 1, rc, rc);
@@ -260,12 +268,16 @@ static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st) {
   return GOFFT_OK;
 }
 
-static int exec_c2r(gofft_plan *p, const void *in, long long nbins, void *out, cudaStream_t st) {
+// adj: the adjoint of the forward -- unnormalised, interior bins halved.
+static int exec_c2r(gofft_plan *p, const void *in, long long nbins, void *out, cudaStream_t st,
+                    bool adj = false) {
   const long long last = p->shape[p->rank - 1], rc = last / 2 + 1;
   if (nbins <= 0 || nbins > rc) nbins = rc;
   if (p->rank == 1) {
-    return p->rx->c2r(mk_side((void *)in, p->idist, 0, p->istride, 1), (int)nbins,
-                      mk_side(out, p->odist, 0, p->ostride, 1), p->batch, 1.0, p->ws, st);
+    // bins on the plan's complex side (odist/ostride), reals on its real side
+    return p->rx->c2r(mk_side((void *)in, p->odist, 0, p->ostride, 1), (int)nbins,
+                      mk_side(out, p->idist, 0, p->istride, 1), p->batch, adj ? (double)last : 1.0, p->ws, st,
+                      adj);
   }
   // 2-D: in (complex) is the plan's output side; out (real) its input side
   const long long rows = p->shape[0], cols = last;
@@ -279,9 +291,11 @@ static int exec_c2r(gofft_plan *p, const void *in, long long nbins, void *out, c
     // columns: complex inverse, normalised by 1/rows (rfft2.go:100-120)
     const Side cin = mk_side((void *)src, rows * rc, 1, rc, rc);
     const Side cout = mk_side(colbuf, rows * rc, 1, rc, rc);
-    if (int e = p->ax[0]->exec(cin, cout, nb * rc, 1, 1, 1.0 / (double)rows, wsx, st)) return e;
+    if (int e = p->ax[0]->exec(cin, cout, nb * rc, 1, 1, adj ? 1.0 : 1.0 / (double)rows, wsx, st)) return e;
     // rows: real inverse of length cols (rfft2.go:122-136)
-    if (int e = p->rx->c2r(contig(colbuf, rc), (int)rc, contig(dst, cols), nb * rows, 1.0, wsx, st)) return e;
+    if (int e = p->rx->c2r(contig(colbuf, rc), (int)rc, contig(dst, cols), nb * rows, adj ? (double)cols : 1.0,
+                           wsx, st, adj))
+      return e;
   }
   return GOFFT_OK;
 }
@@ -777,6 +791,116 @@ extern "C" int gofft_graph_launch(gofft_graph *g, gofft_stream stream) {
 }
 extern "C" int gofft_graph_destroy(gofft_graph *g) {
   delete g;
+  return GOFFT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoints (vector-Jacobian products).  No counterpart in the reference.  The
+// inner product is the real one, Re sum conj(a) b, so a complex gradient
+// holds dL/dRe + i dL/dIm (torch's convention for real losses).
+// ---------------------------------------------------------------------------
+extern "C" int gofft_vjp_c2c(gofft_plan *p, const void *g, void *out, int inverse, gofft_stream stream) {
+  if (!p || !g || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_C2C) return set_err(GOFFT_EINVAL, "plan is not complex-to-complex");
+  // FFT^H = N IFFT = conj(FFT(conj .)) unscaled; IFFT^H = FFT / N.  Both are
+  // the opposite direction with the inverse's scaling.
+  return exec_c2c_dir(p, g, out, inverse ? 0 : 1, inverse ? 1 : 0, (cudaStream_t)stream);
+}
+
+extern "C" int gofft_vjp_r2c(gofft_plan *p, const void *g, void *out, gofft_stream stream) {
+  if (!p || !g || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_R2C) return set_err(GOFFT_EINVAL, "plan is not real");
+  // RFFT^T(G) = N IRFFT(G / w): the unnormalised inverse with interior bins halved
+  return exec_c2r(p, g, 0, out, (cudaStream_t)stream, true);
+}
+
+extern "C" int gofft_vjp_c2r(gofft_plan *p, const void *g, void *out, gofft_stream stream) {
+  if (!p || !g || !out) return set_err(GOFFT_EINVAL, "null argument");
+  if (p->kind != GOFFT_R2C) return set_err(GOFFT_EINVAL, "plan is not real");
+  // IRFFT^T(g) = (w / N) RFFT(g)
+  return exec_r2c(p, g, out, (cudaStream_t)stream, 1.0 / (double)p->total);
+}
+
+// y = IRFFT2(H * RFFT2(x)) per image, and its adjoint, in three passes per L2
+// block of images: rows R2C into the block buffer, one fused column pass
+// (column FFT, multiply, column IFFT -- OpFilterCol) in place, rows C2R.
+static int filter2_run(gofft_plan *p, const void *x, const void *H, void *y, void *saved, void *part, int fl,
+                       cudaStream_t st) {
+  const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
+  const size_t r = rsize(p->prec), c = csize(p->prec);
+  const long long per = rows * rc;
+  char *spec = (char *)p->ws;
+  char *wsx = spec + (((size_t)per * p->chunk * c + 255) & ~(size_t)255);
+  const Exec1D &cx = *p->ax[0];
+  const double dsc = 1.0 / ((double)rows * (double)cols);
+  for (long long b0 = 0; b0 < p->batch; b0 += p->chunk) {
+    const long long nb = std::min(p->chunk, p->batch - b0);
+    const char *src = (const char *)x + (size_t)b0 * rows * cols * r;
+    char *sv = saved ? (char *)saved + (size_t)b0 * per * c : nullptr;
+    char *pt = part ? (char *)part + (size_t)b0 * per * c : nullptr;
+    if (int e = p->rx->r2c(contig((void *)src, cols), contig(spec, rc), nb * rows, wsx, st)) return e;
+    const Side cs = mk_side(spec, per, 1, rc, rc);
+    if (rows > 1 && cx.kind == K_SINGLE) {
+      KArgs a{};
+      a.in = cs;
+      a.out = cs;
+      a.aux0 = H;
+      a.aux1 = sv;
+      a.aux2 = pt;
+      a.ia = cols;
+      a.ic = fl;
+      a.da = dsc;
+      a.cj_out = 1;
+      a.scale = 1.0 / (double)rows;
+      if (int e = launch_line(OP_FILTER_COL, *cx.prog, a, nb * rc, st, 0, true)) return e;
+    } else {
+      if (rows > 1)
+        if (int e = cx.exec(cs, cs, nb * rc, 0, 0, 1.0, wsx, st)) return e;
+      GF_CK(GF_PREC_CALL(p->prec, filter_ew, spec, H, sv, pt, nb, rows, rc, cols, fl, dsc, st));
+      if (rows > 1)
+        if (int e = cx.exec(cs, cs, nb * rc, 1, 1, 1.0 / (double)rows, wsx, st)) return e;
+    }
+    if (y) {
+      char *dst = (char *)y + (size_t)b0 * rows * cols * r;
+      if (int e = p->rx->c2r(contig(spec, rc), (int)rc, contig(dst, cols), nb * rows, 1.0, wsx, st)) return e;
+    }
+  }
+  return GOFFT_OK;
+}
+
+static int filter2_check(gofft_plan *p) {
+  if (!p) return set_err(GOFFT_EINVAL, "null plan");
+  if (p->kind != GOFFT_R2C || p->rank != 2)
+    return set_err(GOFFT_EINVAL, "the 2-D spectral filter needs a rank-2 real plan");
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_filter2_forward(gofft_plan *p, const void *x, const void *H, void *y, void *saved,
+                                     gofft_stream stream) {
+  if (int e = filter2_check(p)) return e;
+  if (!x || !H || !y) return set_err(GOFFT_EINVAL, "null argument");
+  return filter2_run(p, x, H, y, saved, nullptr, saved ? GF_FILT_SAVE : 0, (cudaStream_t)stream);
+}
+
+extern "C" int gofft_vjp_filter2(gofft_plan *p, const void *g, const void *H, const void *saved, void *scratch,
+                                 void *dx, void *dH, gofft_stream stream) {
+  if (int e = filter2_check(p)) return e;
+  if (!g || !H) return set_err(GOFFT_EINVAL, "null argument");
+  if (!dx && !dH) return GOFFT_OK;
+  if (dH && (!saved || !scratch))
+    return set_err(GOFFT_EINVAL, "dH needs the forward's saved spectra and a scratch buffer");
+  const cudaStream_t st = (cudaStream_t)stream;
+  // dx = IRFFT2(conj(H) * RFFT2(g)); dH = sum_b conj(X_b) * (w / (R C)) * RFFT2(g_b)
+  if (dH && saved != scratch) {
+    const size_t bytes = (size_t)p->batch * p->shape[0] * (p->shape[1] / 2 + 1) * csize(p->prec);
+    GF_CK(cudaMemcpyAsync(scratch, saved, bytes, cudaMemcpyDeviceToDevice, st));
+  }
+  const int fl = GF_FILT_CONJ | (dH ? GF_FILT_DH : 0);
+  if (int e = filter2_run(p, g, H, dx, dH ? scratch : nullptr, dH ? scratch : nullptr, fl, st)) return e;
+  if (dH) {
+    const long long count = p->shape[0] * (p->shape[1] / 2 + 1);
+    GF_CK(GF_PREC_CALL(p->prec, sum_batches, dH, scratch, count, p->batch, st));
+  }
   return GOFFT_OK;
 }
 

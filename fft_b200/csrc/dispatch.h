@@ -19,7 +19,8 @@ enum Op {
   OP_RADER_FS1 = 9,   // two-pass Rader: gathered column pass
   OP_RADER_FS2 = 10,  // two-pass Rader: row pass with spectrum multiply
   OP_RADER_FS4 = 11,  // two-pass Rader: row pass with the output scatter
-  OP_COUNT = 12
+  OP_FILTER_COL = 12, // 2-D spectral filter: column FFT, multiply, column IFFT
+  OP_COUNT = 13
 };
 
 typedef void (*KFn)(KArgs);
@@ -66,13 +67,20 @@ struct EwArgs {
   cudaError_t roots(void *tw, long long L, long long count, cudaStream_t st);                 \
   cudaError_t spectrum(void *dst, const double2 *src, double s, long long n, cudaStream_t st); \
   cudaError_t untangle(const Side &dst, const void *Z, long long nl, int m, const void *tw,   \
-                       cudaStream_t st);                                                      \
+                       double wsc, cudaStream_t st);                                          \
   cudaError_t reverse_untangle(void *Z, const Side &src, long long nl, int m, int nb,         \
-                               const void *tw, cudaStream_t st);                              \
+                               const void *tw, int halve, cudaStream_t st);                   \
   cudaError_t promote(void *dst, const Side &src, long long nl, int n, cudaStream_t st);      \
-  cudaError_t copy_bins(const Side &dst, const void *src, long long nl, int n, cudaStream_t st); \
-  cudaError_t mirror(void *dst, const Side &src, long long nl, int n, int nb, cudaStream_t st); \
+  cudaError_t copy_bins(const Side &dst, const void *src, long long nl, int n, double wsc,    \
+                        cudaStream_t st);                                                     \
+  cudaError_t mirror(void *dst, const Side &src, long long nl, int n, int nb, int halve,      \
+                     cudaStream_t st);                                                        \
   cudaError_t take_real(const Side &dst, const void *src, long long nl, int n, double scale,  \
+                        cudaStream_t st);                                                     \
+  cudaError_t sum_batches(void *dst, const void *part, long long count, long long nb,         \
+                          cudaStream_t st);                                                   \
+  cudaError_t filter_ew(void *spec, const void *H, void *saved, void *part, long long nb,     \
+                        long long R, long long K, long long cols, int fl, double dsc,         \
                         cudaStream_t st);                                                     \
   }
 // Plan-time integer and chirp tables (FP64 / exact integer work).

@@ -17,6 +17,7 @@ template <class P, int M, int GROUP> KFn pick_line(int op) {
       case OP_RADER_FS1: return k_line<P, M, OpRaderFS1>;
       case OP_RADER_FS2: return k_line<P, M, OpRaderFS2>;
       case OP_RADER_FS4: return k_line<P, M, OpRaderFS4>;
+      case OP_FILTER_COL: return k_line<P, M, OpFilterCol>;
       default: return nullptr;
     }
   } else {
@@ -165,32 +166,47 @@ static inline int ew_blocks(long long total) {
     return cudaGetLastError();                                                                 \
   }                                                                                            \
   cudaError_t untangle(const Side &dst, const void *Z, long long nl, int m, const void *tw,    \
-                       cudaStream_t st) {                                                      \
+                       double wsc, cudaStream_t st) {                                          \
     k_untangle<C, TW><<<ew_blocks(nl * (m / 2 + 1)), 256, 0, st>>>(dst, (const C *)Z, nl, m, \
-                                                                   (const TW *)tw);            \
+                                                                   (const TW *)tw, wsc);       \
     return cudaGetLastError();                                                                 \
   }                                                                                            \
   cudaError_t reverse_untangle(void *Z, const Side &src, long long nl, int m, int nb,          \
-                               const void *tw, cudaStream_t st) {                              \
+                               const void *tw, int halve, cudaStream_t st) {                   \
     k_reverse_untangle<C, TW><<<ew_blocks(nl * (m / 2 + 1)), 256, 0, st>>>(                   \
-        (C *)Z, src, nl, m, nb, (const TW *)tw);                                               \
+        (C *)Z, src, nl, m, nb, (const TW *)tw, halve);                                        \
     return cudaGetLastError();                                                                 \
   }                                                                                            \
   cudaError_t promote(void *dst, const Side &src, long long nl, int n, cudaStream_t st) {      \
     k_promote<C><<<ew_blocks(nl * n), 256, 0, st>>>((C *)dst, src, nl, n);                    \
     return cudaGetLastError();                                                                 \
   }                                                                                            \
-  cudaError_t copy_bins(const Side &dst, const void *src, long long nl, int n, cudaStream_t st) { \
-    k_copy_bins<C><<<ew_blocks(nl * (n / 2 + 1)), 256, 0, st>>>(dst, (const C *)src, nl, n);  \
+  cudaError_t copy_bins(const Side &dst, const void *src, long long nl, int n, double wsc,     \
+                        cudaStream_t st) {                                                     \
+    k_copy_bins<C><<<ew_blocks(nl * (n / 2 + 1)), 256, 0, st>>>(dst, (const C *)src, nl, n,   \
+                                                                wsc);                          \
     return cudaGetLastError();                                                                 \
   }                                                                                            \
-  cudaError_t mirror(void *dst, const Side &src, long long nl, int n, int nb, cudaStream_t st) { \
-    k_mirror<C><<<ew_blocks(nl * n), 256, 0, st>>>((C *)dst, src, nl, n, nb);                 \
+  cudaError_t mirror(void *dst, const Side &src, long long nl, int n, int nb, int halve,       \
+                     cudaStream_t st) {                                                        \
+    k_mirror<C><<<ew_blocks(nl * n), 256, 0, st>>>((C *)dst, src, nl, n, nb, halve);          \
     return cudaGetLastError();                                                                 \
   }                                                                                            \
   cudaError_t take_real(const Side &dst, const void *src, long long nl, int n, double scale,   \
                         cudaStream_t st) {                                                     \
     k_take_real<C><<<ew_blocks(nl * n), 256, 0, st>>>(dst, (const C *)src, nl, n, scale);     \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t sum_batches(void *dst, const void *part, long long count, long long nb,          \
+                          cudaStream_t st) {                                                   \
+    k_sum_batches<C><<<ew_blocks(count), 256, 0, st>>>((C *)dst, (const C *)part, count, nb); \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t filter_ew(void *spec, const void *H, void *saved, void *part, long long nb,      \
+                        long long R, long long K, long long cols, int fl, double dsc,          \
+                        cudaStream_t st) {                                                     \
+    k_filter_ew<C><<<ew_blocks(nb * R * K), 256, 0, st>>>((C *)spec, (const C *)H, (C *)saved, \
+                                                          (C *)part, nb, R, K, cols, fl, dsc); \
     return cudaGetLastError();                                                                 \
   }                                                                                            \
   }                                                                                            \

@@ -379,6 +379,44 @@ __global__ void k_blue_unchirp(Side dst, const C *y, long long nlines, int n, in
   }
 }
 
+// Elementwise 2-D spectral filter on nb spectra (R x K each, contiguous):
+// the unfused form of OpFilterCol's middle step, Y = X * H (conj(H) with
+// conj_h), optionally saving X and writing the per-image dH terms
+// conj(Xsaved) * G * w_k * dsc (w_k = 1 at k = 0 and 2k = cols, else 2).
+template <class C>
+__global__ void k_filter_ew(C *spec, const C *H, C *saved, C *part, long long nb, long long R, long long K,
+                            long long cols, int fl, double dsc) {
+  using Rl = decltype(C().x);
+  const long long per = R * K, total = nb * per;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long hi = e % per;
+    const long long k = hi % K;
+    const C x = spec[e];
+    if (fl & 2) saved[e] = x;
+    if (fl & 4) {
+      const Rl w = (Rl)(((k == 0 || 2 * k == cols) ? 1.0 : 2.0) * dsc);
+      const C xb = saved[e];
+      part[e] = mkc((xb.x * x.x + xb.y * x.y) * w, (xb.x * x.y - xb.y * x.x) * w);
+    }
+    C h = H[hi];
+    if (fl & 1) h.y = -h.y;
+    spec[e] = cmul(x, h);
+  }
+}
+
+// dH[i] = sum over b of part[b * count + i] (a fixed-order sum, so the
+// parameter gradient is reproducible run to run).
+template <class C>
+__global__ void k_sum_batches(C *dst, const C *part, long long count, long long nb) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x) {
+    C acc = part[i];
+    for (long long b = 1; b < nb; b++) acc = cadd(acc, part[b * count + i]);
+    dst[i] = acc;
+  }
+}
+
 // Copies contiguous lines back to a Side (the inverse of k_gather without
 // permutation), with conjugation and scale.
 template <class C>
@@ -404,11 +442,13 @@ __global__ void k_scatter(Side dst, const C *src, long long nlines, int len, int
 // Untangle of contiguous packed spectra Z (m per line) into bins 0..m of `dst`
 // (realplan.go:138-169).
 template <class C, class TW>
-__global__ void k_untangle(Side dst, const C *Z, long long nlines, int m, const TW *tw) {
+__global__ void k_untangle(Side dst, const C *Z, long long nlines, int m, const TW *tw, double wsc) {
   using Rl = decltype(C().x);
   const int h = m / 2 + 1;
   const long long total = nlines * h;
   const Rl half = (Rl)0.5;
+  // edge-bin weighting of the adjoints: bins 0 and m times wsc, the rest 2 wsc
+  const Rl we = wsc != 0.0 ? (Rl)wsc : (Rl)1, wi = wsc != 0.0 ? (Rl)(2.0 * wsc) : (Rl)1;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const long long l = e / h;
@@ -418,16 +458,17 @@ __global__ void k_untangle(Side dst, const C *Z, long long nlines, int m, const 
     const long long st = dst.stride;
     if (k == 0) {
       C z0 = z[0];
-      o[0] = mkc(z0.x + z0.y, (Rl)0);
-      o[(long long)m * st] = mkc(z0.x - z0.y, (Rl)0);
+      o[0] = mkc((z0.x + z0.y) * we, (Rl)0);
+      o[(long long)m * st] = mkc((z0.x - z0.y) * we, (Rl)0);
       continue;
     }
     C zk = z[k], zm = z[m - k];
     C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
     C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
     C t = twmul(xo, tw[k]);
-    o[(long long)k * st] = cadd(xe, t);
-    if (m - k != k) o[(long long)(m - k) * st] = mkc(xe.x - t.x, t.y - xe.y);
+    const C a = cadd(xe, t);
+    o[(long long)k * st] = mkc(a.x * wi, a.y * wi);
+    if (m - k != k) o[(long long)(m - k) * st] = mkc((xe.x - t.x) * wi, (t.y - xe.y) * wi);
   }
 }
 
@@ -438,18 +479,24 @@ GF_DEV float4 conj_tw(float4 w) { return make_float4(w.x, -w.y, w.z, -w.w); }
 // Reverse untangle (realplan.go:235-272) from bins of `src` (nb per line
 // available) into conjugated packed spectra Z (m per line, contiguous).
 template <class C, class TW>
-__global__ void k_reverse_untangle(C *Z, Side src, long long nlines, int m, int nb, const TW *tw) {
+__global__ void k_reverse_untangle(C *Z, Side src, long long nlines, int m, int nb, const TW *tw,
+                                   int halve) {
   using Rl = decltype(C().x);
   const int h = m / 2 + 1;
   const long long total = nlines * h;
   const Rl half = (Rl)0.5;
+  const Rl wi = halve ? half : (Rl)1;  // adjoints: interior bins enter halved
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const long long l = e / h;
     const int k = (int)(e - l * h);
     const C *in = (const C *)src.ptr + line_off(src, (uint32_t)l);
     const long long st = src.stride;
-    auto bin = [&](int q) -> C { return q < nb ? in[(long long)q * st] : mkc((Rl)0, (Rl)0); };
+    auto bin = [&](int q) -> C {
+      if (q >= nb) return mkc((Rl)0, (Rl)0);
+      const C v = in[(long long)q * st];
+      return (q > 0 && q < m) ? mkc(v.x * wi, v.y * wi) : v;
+    };
     C *z = Z + l * m;
     if (k == 0) {
       const Rl x0 = bin(0).x, xm = bin(m).x;
@@ -480,21 +527,27 @@ __global__ void k_promote(C *dst, Side src, long long nlines, int n) {
 
 // Bins 0..n/2 of contiguous complex lines (n per line) -> dst.
 template <class C>
-__global__ void k_copy_bins(Side dst, const C *src, long long nlines, int n) {
+__global__ void k_copy_bins(Side dst, const C *src, long long nlines, int n, double wsc) {
+  using Rl = decltype(C().x);
   const int h = n / 2 + 1;
   const long long total = nlines * h;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const long long l = e / h;
     const int k = (int)(e - l * h);
-    ((C *)dst.ptr)[line_off(dst, (uint32_t)l) + (long long)k * dst.stride] = src[l * n + k];
+    C v = src[l * n + k];
+    if (wsc != 0.0) {  // edge-bin weighting of the adjoints
+      const Rl w = (Rl)((k == 0 || 2 * k == n) ? wsc : 2.0 * wsc);
+      v = mkc(v.x * w, v.y * w);
+    }
+    ((C *)dst.ptr)[line_off(dst, (uint32_t)l) + (long long)k * dst.stride] = v;
   }
 }
 
 // Hermitian mirror (realplan.go:197-206) of bins (nb available) into
 // conjugated full lines of length n, contiguous.
 template <class C>
-__global__ void k_mirror(C *dst, Side src, long long nlines, int n, int nb) {
+__global__ void k_mirror(C *dst, Side src, long long nlines, int n, int nb, int halve) {
   using Rl = decltype(C().x);
   const int h = n / 2 + 1;
   const long long total = nlines * n;
@@ -511,6 +564,7 @@ __global__ void k_mirror(C *dst, Side src, long long nlines, int n, int nb) {
       const int q = n - i;
       v = q < nb ? in[(long long)q * src.stride] : mkc((Rl)0, (Rl)0);
     }
+    if (halve && i != 0 && 2 * i != n) v = mkc(v.x * (Rl)0.5, v.y * (Rl)0.5);
     dst[e] = v;
   }
 }

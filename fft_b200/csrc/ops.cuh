@@ -16,7 +16,11 @@
 // KArgs::ic bit used by the real-input ops: real pairs are aligned to the
 // pair size, so a pair moves as one vector access.
 #define GF_PAIR_ALIGNED 0x40000000
-#define GF_IC_MASK 0x3fffffff
+// KArgs::ic bit of the real ops: real-spectrum edge-bin weighting for the
+// adjoints -- forward ops multiply bins 0 < k < n/2 (and k = n/2 for odd n)
+// by 2, inverse ops divide them by 2 as they are read.
+#define GF_EDGE_WEIGHT 0x20000000
+#define GF_IC_MASK 0x1fffffff
 
 namespace gf {
 
@@ -181,8 +185,18 @@ struct OpR2CPacked {
   }
   template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
   template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
+    using Rl = typename P::real;
     Cx<P> *out = (Cx<P> *)a.out.ptr;
     const long long st = a.out.stride;
+    if (a.ic & GF_EDGE_WEIGHT) {
+      const int m = a.lp.n;
+      const Rl sc = (Rl)a.scale;
+      untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) {
+        const Rl w = (k == 0 || k == m) ? sc : (Rl)2 * sc;
+        out[base + (long long)k * st] = mkc(v.x * w, v.y * w);
+      }, sb);
+      return;
+    }
     untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) { out[base + (long long)k * st] = v; }, sb);
   }
 };
@@ -233,6 +247,10 @@ struct OpC2RPacked {
         continue;
       }
       C xk = s[k], xmk = s[m - k];
+      if (a.ic & GF_EDGE_WEIGHT) {  // interior bins enter halved (k = m/2 too)
+        xk = mkc(xk.x * half, xk.y * half);
+        xmk = mkc(xmk.x * half, xmk.y * half);
+      }
       // xe = (X[k] + conj X[m-k])/2 ; d = (X[k] - conj X[m-k])/2
       C xe = mkc((xk.x + xmk.x) * half, (xk.y - xmk.y) * half);
       C d = mkc((xk.x - xmk.x) * half, (xk.y + xmk.y) * half);
@@ -268,9 +286,16 @@ struct OpR2CFull {
     if (!c.valid) return mkc((Rl)0, (Rl)0);
     return mkc(((const Rl *)a.in.ptr)[c.ioff + (long long)i * a.in.stride], (Rl)0);
   }
+  template <class P> static GF_DEV Cx<P> weigh(const KArgs &a, int k, Cx<P> y) {
+    using Rl = typename P::real;
+    if (!(a.ic & GF_EDGE_WEIGHT)) return y;
+    const int n = a.lp.n;
+    const Rl w = (Rl)a.scale * ((k == 0 || 2 * k == n) ? (Rl)1 : (Rl)2);
+    return mkc(y.x * w, y.y * w);
+  }
   template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
     if (!c.valid || i > a.lp.n / 2) return;
-    ((Cx<P> *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = y;
+    ((Cx<P> *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = weigh<P>(a, i, y);
   }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     using Rl = typename P::real;
@@ -287,7 +312,7 @@ struct OpR2CFull {
     C *out = (C *)a.out.ptr;
     const int h = a.lp.n / 2 + 1;
     tile_loop(a.out, a.lpc, h, FastDiv((uint32_t)h), a.lpcdiv, line0, a.nlines,
-              [&](int l, int k, long long off) { out[off] = line_view<C>(a, l, sb)[k]; });
+              [&](int l, int k, long long off) { out[off] = weigh<P>(a, k, line_view<C>(a, l, sb)[k]); });
   }
 };
 
@@ -311,6 +336,15 @@ struct OpC2RFull {
     const int n = a.lp.n;
     const int h = n / 2 + 1;
     const int up = n - h;  // mirrored elements i = h .. n-1
+    if (a.ic & GF_EDGE_WEIGHT) {
+      for (int e = threadIdx.x; e < a.lpc * h; e += blockDim.x) {
+        const int l = e / h, i = e - l * h;
+        if (i == 0 || 2 * i == n) continue;
+        const LineView<C> s = line_view<C>(a, l, sb);
+        s[i] = mkc(s[i].x * (typename P::real)0.5, s[i].y * (typename P::real)0.5);
+      }
+      __syncthreads();
+    }
     for (int e = threadIdx.x; e < a.lpc * up; e += blockDim.x) {
       const int l = e / up, i = h + (e - l * up);
       const LineView<C> s = line_view<C>(a, l, sb);
@@ -706,6 +740,69 @@ struct OpRaderFS4 {  // aux0 iperm, aux1 x0s, aux2 dc; ia = q, ib = off
       const C y = cadd(((const C *)a.aux1)[b], cconj(line_view<C>(a, l, sb)[k2]));
       out[base + (long long)__ldg(&((const int *)a.aux0)[qi]) * a.out.stride] = mkc(y.x * sc, y.y * sy);
     }
+  }
+};
+
+
+// ---------------------------------------------------------------------------
+// 2-D spectral filter, column part: for column k of an image's row-transformed
+// spectrum (length R = lp.n, lines = (image b, column k), column-mode sides),
+//   X = FFT_R(column)            (saved to aux1 when GF_FILT_SAVE)
+//   G = X                        (when GF_FILT_DH: dH partial of image b,
+//                                 conj(Xsaved) * w_k * da  -> aux2)
+//   Y = X * H[:, k]              (conj(H) with GF_FILT_CONJ)
+//   out = IFFT_R(Y) * scale      as conj(FFT(conj Y)) / ...
+// H is aux0 (R x K row-major, the data's complex type); ia = C (real row
+// length, for the edge-bin weight w_k = 1 at k = 0 and k = C/2, else 2).
+// This fuses the forward column FFT of RFFT2, the filter multiply and the
+// column IFFT of IRFFT2 (and, for the adjoint, the dH accumulation).
+// ---------------------------------------------------------------------------
+#define GF_FILT_CONJ 1
+#define GF_FILT_SAVE 2
+#define GF_FILT_DH 4
+
+struct OpFilterCol {
+  static constexpr bool kConv = true, kFG = false, kTG = false;
+  static GF_DEV bool first_conj(const KArgs &) { return false; }
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &, const LineCtx &, int) { return Cx<P>(); }
+  template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
+  template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
+    OpC2C::load<P>(a, line0, sb);
+  }
+  template <class P> static GF_DEV void prep(const KArgs &, long long, void * = nullptr) {}
+  template <class P> static GF_DEV void mid(const KArgs &a, long long line0, bool, void *sb = nullptr) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    const C *H = (const C *)a.aux0;
+    C *xs = (C *)a.aux1;
+    C *dh = (C *)a.aux2;
+    const int R = a.lp.n;
+    const int K = (int)a.out.lpb.d;
+    const int Cn = (int)a.ia;
+    tile_loop(a.out, a.lpc, R, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int r, long long off) {
+      uint32_t b, k;
+      a.out.lpb.divmod((uint32_t)(line0 + l), b, k);
+      const LineView<C> s = line_view<C>(a, l, sb);
+      const C x = s[r];
+      const long long hi = (long long)r * K + k;            // H index
+      const long long pi = (long long)b * R * K + hi;       // per-image spectrum index
+      if (a.ic & GF_FILT_SAVE) xs[pi] = x;
+      if (a.ic & GF_FILT_DH) {
+        const Rl w = (k == 0 || 2 * (int)k == Cn) ? (Rl)1 : (Rl)2;
+        const C xb = xs[pi];
+        const Rl sc = w * (Rl)a.da;
+        // conj(Xsaved) * G * w / (R C)
+        dh[pi] = mkc((xb.x * x.x + xb.y * x.y) * sc, (xb.x * x.y - xb.y * x.x) * sc);
+      }
+      C h = H[hi];
+      if (a.ic & GF_FILT_CONJ) h.y = -h.y;
+      s[r] = cconj(cmul(x, h));
+      (void)off;
+    });
+    __syncthreads();
+  }
+  template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
+    OpC2C::store<P>(a, line0, sb);  // conj and 1/R via cj_out and scale
   }
 };
 

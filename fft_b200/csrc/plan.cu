@@ -148,7 +148,7 @@ static size_t max_smem_optin() {
 
 static KFn kernel_for(int prec, int maxe, int op) {
   const bool g0 = op == OP_C2C || op == OP_C2C_TW || op == OP_RADER || op == OP_BLUE || op == OP_RADER_FS1 ||
-                  op == OP_RADER_FS2 || op == OP_RADER_FS4;
+                  op == OP_RADER_FS2 || op == OP_RADER_FS4 || op == OP_FILTER_COL;
   switch (prec) {
     case F64: return g0 ? line_kernel_f64_0(maxe, op) : line_kernel_f64_1(maxe, op);
     case F32: return g0 ? line_kernel_f32_0(maxe, op) : line_kernel_f32_1(maxe, op);
@@ -364,7 +364,7 @@ std::string timing_report() {
 static const char *op_name(int op) {
   static const char *n[] = {"c2c", "c2c_twiddle", "r2c_packed", "c2r_packed", "r2c_full", "c2r_full",
                             "rader_fused", "bluestein_fused", "spectrogram", "rader_fs1", "rader_fs2",
-                            "rader_fs4"};
+                            "rader_fs4", "filter_col"};
   return (op >= 0 && op < OP_COUNT) ? n[op] : "?";
 }
 
@@ -379,6 +379,12 @@ static double algo_bytes(int op, const DevProg &dp, const KArgs &a, long long nl
     case OP_RADER:
     case OP_BLUE: return 2.0 * nl * (double)a.ia * c;
     case OP_SPECTRO: return nl * (2 * n * r + (n + 1) * r);
+    case OP_FILTER_COL: {
+      // spectrum in and out, H read; X saved (forward) or X read and the
+      // per-image dH term written (adjoint)
+      const int extra = ((a.ic & GF_FILT_SAVE) ? 1 : 0) + ((a.ic & GF_FILT_DH) ? 2 : 0);
+      return nl * n * c * (3.0 + extra);
+    }
     default: return 2.0 * nl * n * c;
   }
 }
@@ -459,6 +465,7 @@ static bool side_col(const Side &s) {
   return std::llabs(D) < std::llabs(s.stride);
 }
 int choose_flags(int op, const KArgs &a) {
+  if (op == OP_FILTER_COL) return side_col(a.in) ? GF_COLMAP : 0;
   if (op >= OP_RADER_FS1) return 0;  // gathers and scatters: row layout
   const bool fg = op_fg(op), tg = op_tg(op);
   const bool ic = side_col(a.in), oc = side_col(a.out);
@@ -571,10 +578,6 @@ bool side_simple(const Side &s, long long &D) {
 
 char *align256(char *p) { return (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255); }
 
-#define GF_PREC_CALL(prec, fn, ...)                                                \
-  (count_launch(), (prec) == F64 ? prec_f64::fn(__VA_ARGS__)                       \
-                                 : ((prec) == F32 ? prec_f32::fn(__VA_ARGS__)      \
-                                                  : prec_f32c::fn(__VA_ARGS__)))
 
 int Exec1D::exec(const Side &in, const Side &out, long long nl, int cji, int cjo, double scale,
                  void *ws, cudaStream_t st) const {
@@ -971,7 +974,8 @@ size_t ExecReal::ws_bytes(long long nl) const {
   }
 }
 
-int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaStream_t st) const {
+int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaStream_t st,
+                  double wsc) const {
   if (nl <= 0 || n == 0) return 0;
   const size_t c = csize(prec);
   const long long m = n / 2;
@@ -981,15 +985,16 @@ int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaS
       a.in = in;
       a.out = out;
       a.aux0 = tw2;
-      a.scale = 1.0;
-      a.ic = pairs_aligned(in, prec) ? GF_PAIR_ALIGNED : 0;
+      a.scale = wsc != 0.0 ? wsc : 1.0;
+      a.ic = (pairs_aligned(in, prec) ? GF_PAIR_ALIGNED : 0) | (wsc != 0.0 ? GF_EDGE_WEIGHT : 0);
       return launch_line(OP_R2C, *cx->prog, a, nl, st);
     }
     case R_FULL_FUSED: {
       KArgs a{};
       a.in = in;
       a.out = out;
-      a.scale = 1.0;
+      a.scale = wsc != 0.0 ? wsc : 1.0;
+      a.ic = wsc != 0.0 ? GF_EDGE_WEIGHT : 0;
       return launch_line(OP_R2C_FULL, *cx->prog, a, nl, st);
     }
     case R_PACKED_MULTI: {
@@ -999,7 +1004,7 @@ int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaS
       char *wsub = align256(Z + (size_t)m * nl * c);
       Side zin = mk_side(in.ptr, in.dist_b / 2, in.dist_l / 2, 1, in.lpb.d);
       if (int rc = cx->exec(zin, contig(Z, m), nl, 0, 0, 1.0, wsub, st)) return rc;
-      GF_CK(GF_PREC_CALL(prec, untangle, out, Z, nl, (int)m, tw2, st));
+      GF_CK(GF_PREC_CALL(prec, untangle, out, Z, nl, (int)m, tw2, wsc, st));
       return 0;
     }
     case R_FULL_MULTI: {
@@ -1008,7 +1013,7 @@ int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaS
       char *wsub = align256(B + (size_t)n * nl * c);
       GF_CK(GF_PREC_CALL(prec, promote, A, in, nl, (int)n, st));
       if (int rc = cx->exec(contig(A, n), contig(B, n), nl, 0, 0, 1.0, wsub, st)) return rc;
-      GF_CK(GF_PREC_CALL(prec, copy_bins, out, B, nl, (int)n, st));
+      GF_CK(GF_PREC_CALL(prec, copy_bins, out, B, nl, (int)n, wsc, st));
       return 0;
     }
   }
@@ -1016,7 +1021,7 @@ int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaS
 }
 
 int ExecReal::c2r(const Side &in, int nb, const Side &out, long long nl, double scale, void *ws,
-                  cudaStream_t st) const {
+                  cudaStream_t st, bool halve) const {
   if (nl <= 0 || n == 0) return 0;
   const size_t c = csize(prec);
   const long long m = n / 2;
@@ -1026,7 +1031,7 @@ int ExecReal::c2r(const Side &in, int nb, const Side &out, long long nl, double 
       a.in = in;
       a.out = out;
       a.aux0 = tw2;
-      a.ic = nb | (pairs_aligned(out, prec) ? GF_PAIR_ALIGNED : 0);
+      a.ic = nb | (pairs_aligned(out, prec) ? GF_PAIR_ALIGNED : 0) | (halve ? GF_EDGE_WEIGHT : 0);
       a.scale = scale / (double)m;
       return launch_line(OP_C2R, *cx->prog, a, nl, st);
     }
@@ -1034,7 +1039,7 @@ int ExecReal::c2r(const Side &in, int nb, const Side &out, long long nl, double 
       KArgs a{};
       a.in = in;
       a.out = out;
-      a.ic = nb;
+      a.ic = nb | (halve ? GF_EDGE_WEIGHT : 0);
       a.scale = scale / (double)n;
       return launch_line(OP_C2R_FULL, *cx->prog, a, nl, st);
     }
@@ -1043,7 +1048,7 @@ int ExecReal::c2r(const Side &in, int nb, const Side &out, long long nl, double 
         return set_err(5, "packed real transform needs unit-stride rows with even distances");
       char *Z = align256((char *)ws);
       char *wsub = align256(Z + (size_t)m * nl * c);
-      GF_CK(GF_PREC_CALL(prec, reverse_untangle, Z, in, nl, (int)m, nb, tw2, st));
+      GF_CK(GF_PREC_CALL(prec, reverse_untangle, Z, in, nl, (int)m, nb, tw2, halve ? 1 : 0, st));
       Side zout = mk_side(out.ptr, out.dist_b / 2, out.dist_l / 2, 1, out.lpb.d);
       return cx->exec(contig(Z, m), zout, nl, 0, 1, scale / (double)m, wsub, st);
     }
@@ -1051,7 +1056,7 @@ int ExecReal::c2r(const Side &in, int nb, const Side &out, long long nl, double 
       char *A = align256((char *)ws);
       char *B = A + (size_t)n * nl * c;
       char *wsub = align256(B + (size_t)n * nl * c);
-      GF_CK(GF_PREC_CALL(prec, mirror, A, in, nl, (int)n, nb, st));
+      GF_CK(GF_PREC_CALL(prec, mirror, A, in, nl, (int)n, nb, halve ? 1 : 0, st));
       if (int rc = cx->exec(contig(A, n), contig(B, n), nl, 0, 0, 1.0, wsub, st)) return rc;
       GF_CK(GF_PREC_CALL(prec, take_real, out, B, nl, (int)n, scale / (double)n, st));
       return 0;

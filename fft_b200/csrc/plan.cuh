@@ -96,12 +96,15 @@ struct ExecReal {
   void *tw2 = nullptr;               // W_n^k, k = 0..n/2 (packed modes)
   ~ExecReal();
   size_t ws_bytes(long long nlines) const;
-  // in: reals, out: bins
-  int r2c(const Side &in, const Side &out, long long nlines, void *ws, cudaStream_t st) const;
+  // in: reals, out: bins.  wsc != 0 applies the real-spectrum edge-bin
+  // weighting of the adjoints: bins 0 and n/2 times wsc, the others 2 wsc.
+  int r2c(const Side &in, const Side &out, long long nlines, void *ws, cudaStream_t st,
+          double wsc = 0.0) const;
   // in: bins (nb available per line), out: reals; the result is the
-  // reference-normalised inverse (1/n) times `scale`.
+  // reference-normalised inverse (1/n) times `scale`.  halve: bins other than
+  // 0 and n/2 enter halved (the adjoint of the forward's weighting).
   int c2r(const Side &in, int nb, const Side &out, long long nlines, double scale, void *ws,
-          cudaStream_t st) const;
+          cudaStream_t st, bool halve = false) const;
   std::string describe() const;
 };
 
@@ -117,6 +120,13 @@ bool side_simple(const Side &s, long long &D);
 char *align256(char *p);
 int choose_lpc(const DevProg &dp, const KArgs &a, int op, long long nlines, bool conv);
 int choose_flags(int op, const KArgs &a);
+
+// Calls the elementwise / table function `fn` of a precision's namespace
+// (one counted launch).
+#define GF_PREC_CALL(prec, fn, ...)                                                \
+  (count_launch(), (prec) == F64 ? prec_f64::fn(__VA_ARGS__)                       \
+                                 : ((prec) == F32 ? prec_f32::fn(__VA_ARGS__)      \
+                                                  : prec_f32c::fn(__VA_ARGS__)))
 
 // Launch helper for the line kernels.
 int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st,

@@ -84,6 +84,75 @@ class DevicePlan:
                                    ctypes.c_void_p(out.data_ptr()), _stream(stream)))
         return out
 
+    # adjoints (vector-Jacobian products): real inner product, so a complex
+    # gradient holds dL/dRe + i dL/dIm
+    def vjp_c2c(self, g, out=None, inverse=False, stream=None):
+        _need(g, self.cdtype, "g")
+        if out is None:
+            out = torch.empty_like(g)
+        _need(out, self.cdtype, "out")
+        check(lib().gofft_vjp_c2c(self._h, ctypes.c_void_p(g.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                  1 if inverse else 0, _stream(stream)))
+        return out
+
+    def vjp_r2c(self, g, out=None, stream=None):
+        """Adjoint of r2c: bins -> reals."""
+        _need(g, self.cdtype, "g")
+        if out is None:
+            out = torch.empty((self.batch, self.numel), dtype=self.rdtype, device=g.device)
+        _need(out, self.rdtype, "out")
+        check(lib().gofft_vjp_r2c(self._h, ctypes.c_void_p(g.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                  _stream(stream)))
+        return out
+
+    def vjp_c2r(self, g, out=None, stream=None):
+        """Adjoint of c2r (all bins read): reals -> bins."""
+        _need(g, self.rdtype, "g")
+        if out is None:
+            out = torch.empty((self.batch, self.bins), dtype=self.cdtype, device=g.device)
+        _need(out, self.cdtype, "out")
+        check(lib().gofft_vjp_c2r(self._h, ctypes.c_void_p(g.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                  _stream(stream)))
+        return out
+
+    def filter2(self, x, H, out=None, saved=None, stream=None):
+        """y = IRFFT2(H * RFFT2(x)) per image (rank-2 real plans); saved, if
+        given, receives the spectra RFFT2(x) for the backward's dH."""
+        _need(x, self.rdtype, "x")
+        _need(H, self.cdtype, "H")
+        if out is None:
+            out = torch.empty_like(x)
+        _need(out, self.rdtype, "out")
+        sp = None
+        if saved is not None:
+            _need(saved, self.cdtype, "saved")
+            sp = ctypes.c_void_p(saved.data_ptr())
+        check(lib().gofft_filter2_forward(self._h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(H.data_ptr()),
+                                          ctypes.c_void_p(out.data_ptr()), sp, _stream(stream)))
+        return out
+
+    def vjp_filter2(self, g, H, saved=None, scratch=None, dx=True, dH=True, stream=None):
+        """(dx, dH) of filter2 for the upstream gradient g; either may be
+        skipped.  dH needs the forward's saved spectra; scratch defaults to a
+        fresh buffer (pass saved itself to let it be overwritten)."""
+        _need(g, self.rdtype, "g")
+        _need(H, self.cdtype, "H")
+        ox = torch.empty_like(g) if dx else None
+        oh = torch.empty_like(H) if dH else None
+        sp = sc = None
+        if dH:
+            if saved is None:
+                raise ValueError("dH needs the saved spectra of the forward")
+            _need(saved, self.cdtype, "saved")
+            if scratch is None:
+                scratch = torch.empty_like(saved)
+            _need(scratch, self.cdtype, "scratch")
+            sp, sc = ctypes.c_void_p(saved.data_ptr()), ctypes.c_void_p(scratch.data_ptr())
+        check(lib().gofft_vjp_filter2(self._h, ctypes.c_void_p(g.data_ptr()), ctypes.c_void_p(H.data_ptr()), sp, sc,
+                                      ctypes.c_void_p(ox.data_ptr()) if dx else None,
+                                      ctypes.c_void_p(oh.data_ptr()) if dH else None, _stream(stream)))
+        return ox, oh
+
     # host-pointer variants (copies inside the call): numpy or pinned tensors
     def c2c_host(self, x_ptr, out_ptr, inverse=False):
         check(lib().gofft_exec_c2c_host(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(out_ptr),

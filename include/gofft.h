@@ -228,6 +228,45 @@ GOFFT_API int gofft_graph_launch(gofft_graph *g, gofft_stream stream);
 GOFFT_API int gofft_graph_destroy(gofft_graph *g);
 
 /* ------------------------------------------------------------------------ */
+/* 2d. Adjoints (vector-Jacobian products) and the fused 2-D spectral filter */
+/*     -- no counterpart in the reference, which has no differentiation.     */
+/*     Gradients use the real inner product Re sum conj(a) b: a complex      */
+/*     gradient holds dL/dRe + i dL/dIm (torch.autograd's convention for a   */
+/*     real loss).  Buffers have the layouts of the plan's own transforms.   */
+/* ------------------------------------------------------------------------ */
+
+/* Adjoint of gofft_exec_c2c(p, ., ., inverse): for the forward it is the
+ * unnormalised inverse (N IFFT), for the inverse the forward scaled by 1/N
+ * (N = product of the plan's shape).  g and out: the plan's complex layout. */
+GOFFT_API int gofft_vjp_c2c(gofft_plan *p, const void *g, void *out, int inverse, gofft_stream stream);
+/* Adjoint of gofft_exec_r2c: bins g -> reals out, N IRFFT(g / w) with the
+ * real-spectrum edge-bin weights w_k = 1 for k = 0 and k = n/2 (n even) along
+ * the last axis, 2 otherwise.  Imaginary parts of those edge bins do not
+ * contribute (the forward's outputs there are real for rank 1). */
+GOFFT_API int gofft_vjp_r2c(gofft_plan *p, const void *g, void *out, gofft_stream stream);
+/* Adjoint of gofft_exec_c2r (with all n/2+1 bins read): reals g -> bins out,
+ * (w / N) RFFT(g).  For a short spectrum (nbins < n/2+1) the missing bins'
+ * entries of out are the gradient a caller drops. */
+GOFFT_API int gofft_vjp_c2r(gofft_plan *p, const void *g, void *out, gofft_stream stream);
+
+/* 2-D spectral filter over a rank-2 real plan (batch B of R x C images):
+ *   y_b = IRFFT2(H * RFFT2(x_b)),  H: R x (C/2+1) complex (shared by images).
+ * Three passes per L2 block of images: row R2C, one fused column pass (column
+ * FFT, multiply by H, column IFFT), row C2R.  saved (nullable): B spectra
+ * RFFT2(x_b) written for the backward's dH. */
+GOFFT_API int gofft_filter2_forward(gofft_plan *p, const void *x, const void *H, void *y, void *saved,
+                                    gofft_stream stream);
+/* Backward of gofft_filter2_forward for an upstream gradient g = dL/dy:
+ *   dx   = IRFFT2(conj(H) * RFFT2(g))                      (dx nullable)
+ *   dH   = sum_b conj(X_b) * (w / (R C)) * RFFT2(g_b)      (dH nullable)
+ * with w the edge-bin weights of the C axis.  dH needs the forward's saved
+ * spectra and a scratch buffer of the same size (B R (C/2+1) complex) for the
+ * per-image terms, summed in a fixed order (reproducible); scratch may be
+ * saved itself, which is then overwritten. */
+GOFFT_API int gofft_vjp_filter2(gofft_plan *p, const void *g, const void *H, const void *saved, void *scratch,
+                                void *dx, void *dH, gofft_stream stream);
+
+/* ------------------------------------------------------------------------ */
 /* 3. Instrumentation and tuning (no counterpart in the reference).          */
 /* ------------------------------------------------------------------------ */
 

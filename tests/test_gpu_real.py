@@ -30,6 +30,30 @@ def test_rfft_irfft_f64(n):
     assert rel_l2(d, O.rfft(x)) <= F64_TOL
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32mixed"])
+@pytest.mark.parametrize("n", [1024, 1001, 262144, 12])
+def test_batched_rank1_real_device(prec, n):
+    """Batched 1-D R2C/C2R device plans: bins at n/2+1 per transform, reals
+    at n (each side at its own distance), and a short spectrum (nbins)."""
+    from fft_b200.device import DevicePlan
+    B = 5
+    g = rng(n + 7)
+    x = g.standard_normal((B, n))
+    p = DevicePlan("r2c", prec, [n], batch=B)
+    rdt = torch.float64 if prec == "f64" else torch.float32
+    tol = F64_TOL if prec == "f64" else F32_TOL
+    X = p.r2c(torch.from_numpy(x).to(rdt).cuda())
+    want = np.stack([O.rfft(r) for r in x])
+    assert rel_l2(X.cpu().numpy(), want) <= tol
+    back = p.c2r(X).cpu().numpy()
+    assert rel_l2(back, np.stack([O.irfft(s, n) for s in want])) <= tol
+    k = n // 4 + 1
+    short = X.clone()
+    short[:, k:] = 1e3  # bins past nbins are not read
+    got = p.c2r(short, nbins=k).cpu().numpy()
+    assert rel_l2(got, np.stack([O.irfft(s[:k], n) for s in want])) <= tol
+
+
 def test_irfft_short_and_hermitian():
     # rfft_test.go:105-124, 190-198
     from fft_b200 import gofft as G

@@ -141,3 +141,67 @@ def test_parallel_matches_serial(workers):
     b = O.rfft2(x, 64, 300)
     O.set_workers(0)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("shape", [(16,), (15,), (1,), (2,), (8, 6), (7, 5), (1, 9), (6, 1)])
+def test_adjoint_identities(shape):
+    """The identities the adjoint kernels implement, checked as dot-product
+    tests on the oracle's transforms (real inner product Re sum conj(a) b):
+    RFFT^T(G) = N IRFFT(G / w) and IRFFT^T(g) = (w / N) RFFT(g), w the
+    edge-bin weights of the last axis; FFT^H = N IFFT."""
+    from conftest import edge_weights, rdot, rng
+    g = rng(11)
+    N = int(np.prod(shape))
+    cols = shape[-1]
+    K = cols // 2 + 1
+    bshape = shape[:-1] + (K,)
+    w = edge_weights(cols)
+    if len(shape) == 1:
+        fwd = lambda v: O.rfft(v)
+        inv = lambda S: O.irfft(S, cols)
+    else:
+        fwd = lambda v: O.rfft2(v, *shape).reshape(bshape)
+        inv = lambda S: O.irfft2(S, *shape).reshape(shape)
+    for _ in range(3):
+        x = g.standard_normal(shape)
+        G = g.standard_normal(bshape) + 1j * g.standard_normal(bshape)
+        lhs = rdot(fwd(x), G)
+        rhs = rdot(x, N * inv(G / w))
+        assert abs(lhs - rhs) <= 1e-12 * (abs(lhs) + np.linalg.norm(x) * np.linalg.norm(G))
+        y = g.standard_normal(shape)
+        lhs = rdot(inv(G), y)
+        rhs = rdot(G, w / N * fwd(y))
+        assert abs(lhs - rhs) <= 1e-12 * (abs(lhs) + np.linalg.norm(y) * np.linalg.norm(G))
+    z = g.standard_normal(N) + 1j * g.standard_normal(N)
+    Z = g.standard_normal(N) + 1j * g.standard_normal(N)
+    cs = list(shape)
+    assert abs(rdot(O.fftn(z, cs), Z) - rdot(z, N * O.ifftn(Z, cs))) <= 1e-12 * N * np.linalg.norm(z) * np.linalg.norm(Z)
+
+
+def test_filter_gradient_identity():
+    """dx and dH of L = sum(y^2), y = IRFFT2(H * RFFT2(x)), as assembled from
+    the oracle's transforms, against central differences on a small case
+    (L is quadratic, so the central difference is exact up to rounding)."""
+    from conftest import filter_case, filter_oracle, rng
+    x, H = filter_case(batch=2, rows=6, cols=8)
+    x = x.astype(np.float64)
+    H = H.astype(np.complex128)
+    y, dx, dH = filter_oracle(x, H)
+    loss = lambda xx, HH: float(np.sum(filter_oracle(xx, HH)[0] ** 2))
+    e = 1e-6
+    g = rng(3)
+    for _ in range(8):
+        b, i, j = g.integers(0, 2), g.integers(0, 6), g.integers(0, 8)
+        xp, xm = x.copy(), x.copy()
+        xp[b, i, j] += e
+        xm[b, i, j] -= e
+        fd = (loss(xp, H) - loss(xm, H)) / (2 * e)
+        assert abs(fd - dx[b, i, j]) <= 1e-6 * (1 + abs(dx[b, i, j]))
+        r, k = g.integers(0, 6), g.integers(0, 5)
+        for unit in (1.0, 1j):
+            Hp, Hm = H.copy(), H.copy()
+            Hp[r, k] += e * unit
+            Hm[r, k] -= e * unit
+            fd = (loss(x, Hp) - loss(x, Hm)) / (2 * e)
+            want = dH[r, k].real if unit == 1.0 else dH[r, k].imag
+            assert abs(fd - want) <= 1e-6 * (1 + abs(want))
