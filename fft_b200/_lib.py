@@ -82,6 +82,8 @@ SIGNATURES = {
     "gofft_timing_report": (_i64, [ctypes.c_char_p, _i64]),
     "gofft_set_lines_per_cta": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gofft_set_pipelined": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int]),
+    "gofft_set_schedule": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int]),
+    "gofft_get_schedule": (ctypes.c_int, [ctypes.c_int, _i64]),
 }
 
 _lib = None

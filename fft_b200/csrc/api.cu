@@ -25,6 +25,10 @@ struct gofft_plan {
   std::vector<std::shared_ptr<const Exec1D>> ax;  // complex exec per axis
   std::shared_ptr<const ExecReal> rx;             // real exec of the last axis (R2C)
   long long chunk = 1;                            // images per L2 block (rank-2 R2C)
+  int nlanes = 1;                                 // streams the blocks alternate on
+  size_t lane_bytes = 0;                          // workspace per lane
+  cudaStream_t lane = nullptr;                    // the second lane's stream
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   size_t ws_bytes = 0;
   void *ws = nullptr;
   void *d_in = nullptr, *d_out = nullptr;
@@ -38,6 +42,9 @@ struct gofft_plan {
     if (d_in) cudaFree(d_in);
     if (d_out) cudaFree(d_out);
     if (stream) cudaStreamDestroy(stream);
+    if (lane) cudaStreamDestroy(lane);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 };
 
@@ -71,9 +78,12 @@ static int plan_ws(gofft_plan *p) {
   } else if (p->rank == 1) {
     need = p->rx->ws_bytes(p->batch);
   } else {
+    // per lane: the block's spectrum buffer, then the passes' own workspace
     const long long rows = p->shape[0], rc = p->shape[1] / 2 + 1;
-    const size_t cols_buf = (size_t)rows * rc * p->chunk * csize(p->prec) + 256;
-    need = cols_buf + std::max(p->rx->ws_bytes(rows * p->chunk), p->ax[0]->ws_bytes(rc * p->chunk));
+    const size_t cols_buf = ((size_t)rows * rc * p->chunk * csize(p->prec) + 255) & ~(size_t)255;
+    const size_t sub = std::max(p->rx->ws_bytes(rows * p->chunk), p->ax[0]->ws_bytes(rc * p->chunk));
+    p->lane_bytes = (cols_buf + sub + 255) & ~(size_t)255;
+    need = p->lane_bytes * p->nlanes;
   }
   p->ws_bytes = need;
   if (need) {
@@ -135,10 +145,18 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       const long long cmax = std::max<long long>(1, std::min<long long>(batch, budget / std::max<long long>(1, per)));
       const long long nblocks = (batch + cmax - 1) / cmax;
       p->chunk = (batch + nblocks - 1) / nblocks;  // balanced blocks
+      // two lanes: block i+1's passes overlap block i's (each pass alone
+      // ramps up and drains; the other lane fills those gaps)
+      if (nblocks > 1 && env_ll("GOFFT_LANES", 2) >= 2) p->nlanes = 2;
     }
   }
   if (int rc2 = plan_ws(p.get())) return rc2;
   GF_CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  if (p->nlanes > 1) {
+    GF_CK(cudaStreamCreateWithFlags(&p->lane, cudaStreamNonBlocking));
+    GF_CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+    GF_CK(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
+  }
   *out = p.release();
   return GOFFT_OK;
 }
@@ -243,6 +261,41 @@ static int exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, cudaS
   return exec_c2c_dir(p, in, out, inverse ? 1 : 0, inverse ? 1 : 0, st);
 }
 
+// The L2 blocks of a rank-2 real plan alternate between the caller's stream
+// and the plan's lane stream (forked from and joined back into the caller's
+// stream), each lane with its own workspace region: block spectrum buffer
+// first, then the passes' workspace.
+struct Lanes {
+  gofft_plan *p;
+  cudaStream_t st;
+  bool two = false;
+  Lanes(gofft_plan *p_, cudaStream_t st_) : p(p_), st(st_) {}
+  int fork() {
+    two = p->nlanes > 1 && p->chunk < p->batch;
+    if (!two) return 0;
+    GF_CK(cudaEventRecord(p->ev_fork, st));
+    GF_CK(cudaStreamWaitEvent(p->lane, p->ev_fork, 0));
+    return 0;
+  }
+  cudaStream_t stream(long long blk) const { return (two && (blk & 1)) ? p->lane : st; }
+  char *buf(long long blk) const { return (char *)p->ws + ((two && (blk & 1)) ? p->lane_bytes : 0); }
+  char *sub(long long blk) const {
+    const long long rows = p->shape[0], rc = p->shape[1] / 2 + 1;
+    return buf(blk) + (((size_t)rows * rc * p->chunk * csize(p->prec) + 255) & ~(size_t)255);
+  }
+  // Joins the lane back into the caller's stream; keeps the first error.
+  int join(int rc) {
+    if (!two) return rc;
+    two = false;
+    cudaError_t e1 = cudaEventRecord(p->ev_join, p->lane);
+    cudaError_t e2 = cudaStreamWaitEvent(st, p->ev_join, 0);
+    if (rc) return rc;
+    if (e1 != cudaSuccess || e2 != cudaSuccess)
+      return set_err(GOFFT_ECUDA, std::string("lane join: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    return 0;
+  }
+};
+
 // wsc != 0: the adjoint of the inverse (edge-bin weighting with scale wsc on
 // the row pass, the only real one).
 static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st, double wsc = 0.0) {
@@ -252,20 +305,24 @@ static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st, d
   }
   const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
   const size_t r = rsize(p->prec), c = csize(p->prec);
-  char *wsx = (char *)p->ws + (((size_t)rows * rc * p->chunk * c + 255) & ~(size_t)255);
-  for (long long b0 = 0; b0 < p->batch; b0 += p->chunk) {
+  Lanes ln(p, st);
+  if (int e = ln.fork()) return e;
+  long long blk = 0;
+  for (long long b0 = 0; b0 < p->batch; b0 += p->chunk, blk++) {
     const long long nb = std::min(p->chunk, p->batch - b0);
     const char *src = (const char *)in + (size_t)b0 * rows * cols * r;
     char *dst = (char *)out + (size_t)b0 * rows * rc * c;
+    const cudaStream_t s = ln.stream(blk);
+    char *wsx = ln.sub(blk);
     // rows: real transform along the last axis (rfft2.go:41-51)
-    if (int e = p->rx->r2c(contig((void *)src, cols), contig(dst, rc), nb * rows, wsx, st, wsc)) return e;
+    if (int e = p->rx->r2c(contig((void *)src, cols), contig(dst, rc), nb * rows, wsx, s, wsc)) return ln.join(e);
     // columns: complex transform down each of the rc columns (rfft2.go:53-72)
     if (rows > 1) {
       const Side cs = mk_side(dst, rows * rc, 1, rc, rc);
-      if (int e = p->ax[0]->exec(cs, cs, nb * rc, 0, 0, 1.0, wsx, st)) return e;
+      if (int e = p->ax[0]->exec(cs, cs, nb * rc, 0, 0, 1.0, wsx, s)) return ln.join(e);
     }
   }
-  return GOFFT_OK;
+  return ln.join(GOFFT_OK);
 }
 
 // adj: the adjoint of the forward -- unnormalised, interior bins halved.
@@ -282,22 +339,27 @@ static int exec_c2r(gofft_plan *p, const void *in, long long nbins, void *out, c
   // 2-D: in (complex) is the plan's output side; out (real) its input side
   const long long rows = p->shape[0], cols = last;
   const size_t r = rsize(p->prec), c = csize(p->prec);
-  char *colbuf = (char *)p->ws;
-  char *wsx = colbuf + (((size_t)rows * rc * p->chunk * c + 255) & ~(size_t)255);
-  for (long long b0 = 0; b0 < p->batch; b0 += p->chunk) {
+  Lanes ln(p, st);
+  if (int e = ln.fork()) return e;
+  long long blk = 0;
+  for (long long b0 = 0; b0 < p->batch; b0 += p->chunk, blk++) {
     const long long nb = std::min(p->chunk, p->batch - b0);
     const char *src = (const char *)in + (size_t)b0 * rows * rc * c;
     char *dst = (char *)out + (size_t)b0 * rows * cols * r;
+    const cudaStream_t s = ln.stream(blk);
+    char *colbuf = ln.buf(blk);
+    char *wsx = ln.sub(blk);
     // columns: complex inverse, normalised by 1/rows (rfft2.go:100-120)
     const Side cin = mk_side((void *)src, rows * rc, 1, rc, rc);
     const Side cout = mk_side(colbuf, rows * rc, 1, rc, rc);
-    if (int e = p->ax[0]->exec(cin, cout, nb * rc, 1, 1, adj ? 1.0 : 1.0 / (double)rows, wsx, st)) return e;
+    if (int e = p->ax[0]->exec(cin, cout, nb * rc, 1, 1, adj ? 1.0 : 1.0 / (double)rows, wsx, s))
+      return ln.join(e);
     // rows: real inverse of length cols (rfft2.go:122-136)
     if (int e = p->rx->c2r(contig(colbuf, rc), (int)rc, contig(dst, cols), nb * rows, adj ? (double)cols : 1.0,
-                           wsx, st, adj))
-      return e;
+                           wsx, s, adj))
+      return ln.join(e);
   }
-  return GOFFT_OK;
+  return ln.join(GOFFT_OK);
 }
 
 extern "C" int gofft_exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, gofft_stream stream) {
@@ -759,6 +821,15 @@ extern "C" int gofft_set_pipelined(int precision, int64_t n, int op, int on) {
   return GOFFT_OK;
 }
 
+extern "C" int gofft_set_schedule(int precision, int64_t n, int variant) {
+  if (precision < 0 || precision > 2 || n < 1 || variant < 0 || variant > 1)
+    return set_err(GOFFT_EINVAL, "bad schedule override");
+  set_sched_variant(precision, n, variant);
+  return GOFFT_OK;
+}
+
+extern "C" int gofft_get_schedule(int precision, int64_t n) { return get_sched_variant(precision, n); }
+
 // ---------------------------------------------------------------------------
 // CUDA graphs
 // ---------------------------------------------------------------------------
@@ -829,16 +900,21 @@ static int filter2_run(gofft_plan *p, const void *x, const void *H, void *y, voi
   const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
   const size_t r = rsize(p->prec), c = csize(p->prec);
   const long long per = rows * rc;
-  char *spec = (char *)p->ws;
-  char *wsx = spec + (((size_t)per * p->chunk * c + 255) & ~(size_t)255);
   const Exec1D &cx = *p->ax[0];
   const double dsc = 1.0 / ((double)rows * (double)cols);
+  Lanes ln(p, st);
+  if (int e = ln.fork()) return e;
+  long long blk = -1;
   for (long long b0 = 0; b0 < p->batch; b0 += p->chunk) {
+    blk++;
     const long long nb = std::min(p->chunk, p->batch - b0);
+    const cudaStream_t s = ln.stream(blk);
+    char *spec = ln.buf(blk);
+    char *wsx = ln.sub(blk);
     const char *src = (const char *)x + (size_t)b0 * rows * cols * r;
     char *sv = saved ? (char *)saved + (size_t)b0 * per * c : nullptr;
     char *pt = part ? (char *)part + (size_t)b0 * per * c : nullptr;
-    if (int e = p->rx->r2c(contig((void *)src, cols), contig(spec, rc), nb * rows, wsx, st)) return e;
+    if (int e = p->rx->r2c(contig((void *)src, cols), contig(spec, rc), nb * rows, wsx, s)) return ln.join(e);
     const Side cs = mk_side(spec, per, 1, rc, rc);
     if (rows > 1 && cx.kind == K_SINGLE) {
       KArgs a{};
@@ -852,20 +928,21 @@ static int filter2_run(gofft_plan *p, const void *x, const void *H, void *y, voi
       a.da = dsc;
       a.cj_out = 1;
       a.scale = 1.0 / (double)rows;
-      if (int e = launch_line(OP_FILTER_COL, *cx.prog, a, nb * rc, st, 0, true)) return e;
+      if (int e = launch_line(OP_FILTER_COL, *cx.prog, a, nb * rc, s, 0, true)) return ln.join(e);
     } else {
       if (rows > 1)
-        if (int e = cx.exec(cs, cs, nb * rc, 0, 0, 1.0, wsx, st)) return e;
-      GF_CK(GF_PREC_CALL(p->prec, filter_ew, spec, H, sv, pt, nb, rows, rc, cols, fl, dsc, st));
+        if (int e = cx.exec(cs, cs, nb * rc, 0, 0, 1.0, wsx, s)) return ln.join(e);
+      if (GF_PREC_CALL(p->prec, filter_ew, spec, H, sv, pt, nb, rows, rc, cols, fl, dsc, s) != cudaSuccess)
+        return ln.join(set_err(GOFFT_ECUDA, "filter kernel launch failed"));
       if (rows > 1)
-        if (int e = cx.exec(cs, cs, nb * rc, 1, 1, 1.0 / (double)rows, wsx, st)) return e;
+        if (int e = cx.exec(cs, cs, nb * rc, 1, 1, 1.0 / (double)rows, wsx, s)) return ln.join(e);
     }
     if (y) {
       char *dst = (char *)y + (size_t)b0 * rows * cols * r;
-      if (int e = p->rx->c2r(contig(spec, rc), (int)rc, contig(dst, cols), nb * rows, 1.0, wsx, st)) return e;
+      if (int e = p->rx->c2r(contig(spec, rc), (int)rc, contig(dst, cols), nb * rows, 1.0, wsx, s)) return ln.join(e);
     }
   }
-  return GOFFT_OK;
+  return ln.join(GOFFT_OK);
 }
 
 static int filter2_check(gofft_plan *p) {

@@ -67,6 +67,48 @@ GF_DEV float2 twmul(float2 a, float4 w) {
   im = fmaf(a.x, w.y, fmaf(a.y, w.x, im));
   return mkc(re, im);
 }
+// Cache-hinted global loads.  Line data is read once per pass: it is not
+// allocated in L1 (ld_stream), so the small tables every line rereads
+// (stage twiddles, untangle roots) keep their L1 lines; those tables are
+// read-only for the kernel's lifetime and loaded with L1 priority (ld_keep).
+GF_DEV double2 ld_stream(const double2 *p) {
+  double2 v;
+  asm("ld.global.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+GF_DEV float2 ld_stream(const float2 *p) {
+  float2 v;
+  asm("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+GF_DEV double ld_stream(const double *p) {
+  double v;
+  asm("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+GF_DEV float ld_stream(const float *p) {
+  float v;
+  asm("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+GF_DEV double2 ld_keep(const double2 *p) {
+  double2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+GF_DEV float2 ld_keep(const float2 *p) {
+  float2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+GF_DEV float4 ld_keep(const float4 *p) {
+  float4 v;
+  asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "l"(p));
+  return v;
+}
+
 // Spectrum multiply (Rader / Bluestein convolution): always FP64-derived.
 GF_DEV double2 spmul(double2 a, double2 w) { return cmul(a, w); }
 GF_DEV float2 spmul(float2 a, float4 w) { return twmul(a, w); }

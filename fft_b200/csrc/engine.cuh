@@ -197,7 +197,7 @@ GF_DEV void stage(typename P::cpx (&v)[MAXE], const LineView<typename P::cpx> &s
       if (ns > 1) {
 #pragma unroll
         for (int r = 1; r < R; r++)
-          v[b * R + r] = twmul(v[b * R + r], __ldg(&tw[(r - 1) * ns + k]));
+          v[b * R + r] = twmul(v[b * R + r], ld_keep(&tw[(r - 1) * ns + k]));
       }
       Dft<R, C>::run(&v[b * R]);
       const int base = (int)q * ns * R + (int)k;
@@ -361,7 +361,7 @@ GF_DEV void stage_ct(typename P::cpx (&v)[E], const LineView<typename P::cpx> &s
       if constexpr (NS > 1) {
 #pragma unroll
         for (int r = 1; r < R; r++)
-          v[b * R + r] = twmul(v[b * R + r], __ldg(&tw[(r - 1) * NS + k]));
+          v[b * R + r] = twmul(v[b * R + r], ld_keep(&tw[(r - 1) * NS + k]));
       }
       Dft<R, C>::run(&v[b * R]);
       const int base = q * NS * R + k;

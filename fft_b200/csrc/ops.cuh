@@ -34,8 +34,8 @@ GF_DEV float4 cconj_tw(float4 w) { return make_float4(w.x, -w.y, w.z, -w.w); }
 template <class P> GF_DEV Cx<P> read_pair(const KArgs &a, long long base, long long st) {
   using Rl = typename P::real;
   const Rl *in = (const Rl *)a.in.ptr;
-  if (a.ic & GF_PAIR_ALIGNED) return *reinterpret_cast<const Cx<P> *>(&in[base]);
-  return mkc(in[base], in[base + st]);
+  if (a.ic & GF_PAIR_ALIGNED) return ld_stream(reinterpret_cast<const Cx<P> *>(&in[base]));
+  return mkc(ld_stream(&in[base]), ld_stream(&in[base + st]));
 }
 
 // Copies the real pair (x[base], x[base + st]) into a complex slot.
@@ -73,7 +73,7 @@ struct OpC2C {
   template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int i) {
     using Rl = typename P::real;
     if (!c.valid) return mkc((Rl)0, (Rl)0);
-    return ((const Cx<P> *)a.in.ptr)[c.ioff + (long long)i * a.in.stride];
+    return ld_stream(&((const Cx<P> *)a.in.ptr)[c.ioff + (long long)i * a.in.stride]);
   }
   template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
     using Rl = typename P::real;
@@ -115,7 +115,7 @@ struct OpC2CTwiddle {
     uint32_t b, n2;
     a.out.lpb.divmod((uint32_t)line, b, n2);
     const long long e = ((long long)n2 * i) % a.ia;
-    return twmul(y, __ldg(&((const TW *)a.aux0)[e]));
+    return twmul(y, ld_keep(&((const TW *)a.aux0)[e]));
   }
   template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
     if (!c.valid) return;
@@ -161,7 +161,7 @@ GF_DEV void untangle_tile(const KArgs &a, long long line0, F emit, void *sb) {
               C zk = s[k], zm = s[m - k];
               C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
               C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
-              C t = twmul(xo, __ldg(&tw[k]));
+              C t = twmul(xo, ld_keep(&tw[k]));
               emit(base, k, cadd(xe, t));
               if (m - k != k) emit(base, m - k, mkc(xe.x - t.x, t.y - xe.y));
             });
@@ -254,7 +254,7 @@ struct OpC2RPacked {
       // xe = (X[k] + conj X[m-k])/2 ; d = (X[k] - conj X[m-k])/2
       C xe = mkc((xk.x + xmk.x) * half, (xk.y - xmk.y) * half);
       C d = mkc((xk.x - xmk.x) * half, (xk.y + xmk.y) * half);
-      C xo = twmul(d, cconj_tw(__ldg(&tw[k])));
+      C xo = twmul(d, cconj_tw(ld_keep(&tw[k])));
       // Z[k] = xe + i xo ; Z[m-k] = conj(xe - i xo); stored conjugated
       s[k] = cconj(mkc(xe.x - xo.y, xe.y + xo.x));
       if (m - k != k) s[m - k] = cconj(mkc(xe.x + xo.y, -(xe.y - xo.x)));
@@ -284,7 +284,7 @@ struct OpR2CFull {
   template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int i) {
     using Rl = typename P::real;
     if (!c.valid) return mkc((Rl)0, (Rl)0);
-    return mkc(((const Rl *)a.in.ptr)[c.ioff + (long long)i * a.in.stride], (Rl)0);
+    return mkc(ld_stream(&((const Rl *)a.in.ptr)[c.ioff + (long long)i * a.in.stride]), (Rl)0);
   }
   template <class P> static GF_DEV Cx<P> weigh(const KArgs &a, int k, Cx<P> y) {
     using Rl = typename P::real;
@@ -496,7 +496,7 @@ struct OpBluestein {
     using Rl = typename P::real;
     using SP = typename P::sp_t;
     if (!c.valid || j >= (int)a.ia) return mkc((Rl)0, (Rl)0);
-    C v = ((const C *)a.in.ptr)[c.ioff + (long long)j * a.in.stride];
+    C v = ld_stream(&((const C *)a.in.ptr)[c.ioff + (long long)j * a.in.stride]);
     if (a.cj_in) v.y = -v.y;
     return spmul(v, __ldg(&((const SP *)a.aux0)[j]));
   }

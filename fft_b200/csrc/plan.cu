@@ -106,16 +106,38 @@ long long best_conv_len(long long lo) {
   return best;
 }
 
+// Schedule variants per (precision, length): 0 = radices up to 16 with 16
+// (FP64) or up to 32 (FP32) elements per thread; 1 = radices up to 8 with 8
+// elements per thread (twice the threads per line, about half the registers,
+// more resident warps, one more stage).  Objects built under one setting are
+// cached apart from those built under another (the epoch is part of every
+// cache key).
+static std::mutex g_sched_mu;
+static std::map<std::pair<int, long long>, int> g_sched;
+static std::atomic<int> g_sched_epoch{0};
+void set_sched_variant(int prec, long long n, int v) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  if (v <= 0) g_sched.erase(std::make_pair(prec, n));
+  else g_sched[std::make_pair(prec, n)] = v;
+  g_sched_epoch.fetch_add(1);
+}
+int get_sched_variant(int prec, long long n) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  auto it = g_sched.find(std::make_pair(prec, n));
+  return it == g_sched.end() ? 0 : it->second;
+}
+int sched_epoch() { return g_sched_epoch.load(); }
+
 // Radix schedule of a 13-smooth length for the Stockham stages: the power of
-// two is split into as few radix-16/8/4/2 stages as possible with the bits
-// spread evenly, then one stage per odd prime factor.
-std::vector<int> gpu_radices(long long n) {
+// two is split into as few stages of radix at most 2^maxlog as possible with
+// the bits spread evenly, then one stage per odd prime factor.
+std::vector<int> gpu_radices(long long n, int maxlog) {
   std::vector<int> r;
   long long m = n;
   int a = 0;
   while (m % 2 == 0) { a++; m /= 2; }
   if (a > 0) {
-    int k = (a + 3) / 4;
+    int k = (a + maxlog - 1) / maxlog;
     for (int i = 0; i < k; i++) r.push_back(1 << (a / k + (i < a % k ? 1 : 0)));
   }
   for (int p : {3, 5, 7, 11, 13})
@@ -218,10 +240,19 @@ static int pick_threads(long long n, int maxe, const std::vector<int> &rad) {
 
 static bool schedule_for(long long n, int prec, int &maxe, int &T, std::vector<int> &rad) {
   if (n < 1 || !smooth13(n)) return false;
-  rad = gpu_radices(n);
-  if ((int)rad.size() > GF_MAXST) return false;
   const size_t bytes = (size_t)spad_size((int)n) * csize(prec) + 2 * csize(prec);
   if (bytes > max_smem_optin()) return false;
+  if (get_sched_variant(prec, n) == 1) {
+    rad = gpu_radices(n, 3);
+    const int t = (int)rad.size() <= GF_MAXST ? pick_threads(n, 8, rad) : -1;
+    if (t > 0) {
+      maxe = 8;
+      T = t;
+      return true;
+    }
+  }
+  rad = gpu_radices(n, 4);
+  if ((int)rad.size() > GF_MAXST) return false;
   for (int me : {16, 32}) {
     if (me == 32 && prec == F64) break;
     const int t = pick_threads(n, me, rad);
@@ -290,9 +321,8 @@ static int build_prog(long long n, int prec, std::shared_ptr<DevProg> &out) {
   return 0;
 }
 
-template <class V>
-static std::shared_ptr<V> cache_get(std::map<std::tuple<int, long long, int>, std::shared_ptr<V>> &c,
-                                    std::mutex &mu, const std::tuple<int, long long, int> &k) {
+template <class K, class V>
+static std::shared_ptr<V> cache_get(std::map<K, std::shared_ptr<V>> &c, std::mutex &mu, const K &k) {
   std::lock_guard<std::mutex> lk(mu);
   auto it = c.find(k);
   return it == c.end() ? nullptr : it->second;
@@ -300,8 +330,8 @@ static std::shared_ptr<V> cache_get(std::map<std::tuple<int, long long, int>, st
 
 std::shared_ptr<DevProg> get_prog(long long n, int prec) {
   static std::mutex mu;
-  static std::map<std::tuple<int, long long, int>, std::shared_ptr<DevProg>> cache;
-  auto key = std::make_tuple(cur_device(), n, prec);
+  static std::map<std::tuple<int, long long, int, int>, std::shared_ptr<DevProg>> cache;
+  auto key = std::make_tuple(cur_device(), n, prec, sched_epoch());
   if (auto p = cache_get(cache, mu, key)) return p;
   std::shared_ptr<DevProg> p;
   if (build_prog(n, prec, p) != 0) return nullptr;
@@ -944,8 +974,8 @@ static int build_exec(long long n, int prec, std::shared_ptr<Exec1D> &out) {
 
 std::shared_ptr<const Exec1D> get_exec(long long n, int prec) {
   static std::mutex mu;
-  static std::map<std::tuple<int, long long, int>, std::shared_ptr<Exec1D>> cache;
-  auto key = std::make_tuple(cur_device(), n, prec);
+  static std::map<std::tuple<int, long long, int, int>, std::shared_ptr<Exec1D>> cache;
+  auto key = std::make_tuple(cur_device(), n, prec, sched_epoch());
   if (auto p = cache_get(cache, mu, key)) return p;
   // built outside the lock: prime lengths re-enter get_exec for their
   // convolution (the reference's cachedPlan does the same, plan.go:295-300)
@@ -1096,8 +1126,8 @@ static int build_real(long long n, int prec, std::shared_ptr<ExecReal> &out) {
 
 std::shared_ptr<const ExecReal> get_real(long long n, int prec) {
   static std::mutex mu;
-  static std::map<std::tuple<int, long long, int>, std::shared_ptr<ExecReal>> cache;
-  auto key = std::make_tuple(cur_device(), n, prec);
+  static std::map<std::tuple<int, long long, int, int>, std::shared_ptr<ExecReal>> cache;
+  auto key = std::make_tuple(cur_device(), n, prec, sched_epoch());
   if (auto p = cache_get(cache, mu, key)) return p;
   std::shared_ptr<ExecReal> p;
   if (build_real(n, prec, p) != 0) return nullptr;

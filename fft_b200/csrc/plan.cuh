@@ -41,7 +41,12 @@ bool is_prime_ll(long long n);
 long long primitive_root_ll(long long p);
 bool conv_cost(long long m, double *cost);
 long long best_conv_len(long long lo);
-std::vector<int> gpu_radices(long long n);
+// Power-of-two part split into near-equal radices of at most 2^maxlog,
+// then the odd primes.
+std::vector<int> gpu_radices(long long n, int maxlog = 4);
+void set_sched_variant(int prec, long long n, int v);
+int get_sched_variant(int prec, long long n);
+int sched_epoch();
 
 struct DevProg {
   int n = 0, prec = 0, maxe = 16, device = 0;

@@ -6,8 +6,8 @@
  *  1. The reference-facing entry points (gofft_new_plan ... gofft_spectrogram)
  *     mirror the Go API one call for one call: host buffers of complex128
  *     (interleaved re,im doubles) or float64, one transform per call, the same
- *     argument meaning and normalisation.  A cgo binding calls these (see
- *     INTEGRATION.md).  Argument errors that the Go API turns into a panic
+ *     argument meaning and normalisation.  A cgo binding calls these.
+ *     Argument errors that the Go API turns into a panic
  *     return GOFFT_EINVAL with the reference's panic text in
  *     gofft_last_error().
  *
@@ -286,6 +286,13 @@ GOFFT_API int gofft_set_lines_per_cta(int precision, int64_t n, int op, int colm
 /* Selects (on = 1) the persistent double-buffered line kernel for
  * (precision, n, op) where one exists.  Used by the autotuner. */
 GOFFT_API int gofft_set_pipelined(int precision, int64_t n, int op, int on);
+/* Radix-schedule variant of length n in a precision, for plans created
+ * afterwards (plans already created keep theirs): 0 = radices up to 16 with
+ * 16 elements per thread (FP32: up to 32), the default; 1 = radices up to 8
+ * with 8 elements per thread (twice the threads per line, half the
+ * registers, one more stage).  The autotuner's schedule choice. */
+GOFFT_API int gofft_set_schedule(int precision, int64_t n, int variant);
+GOFFT_API int gofft_get_schedule(int precision, int64_t n);
 
 #ifdef __cplusplus
 }
