@@ -250,6 +250,21 @@ def run_ours(args):
     B = args.batch
     peak, peak_kind = peaks()
 
+    # the engine's own autotuner picks radix schedules and lines per CTA for
+    # this shape (setup, before any timed work)
+    from fft_b200 import tune
+    tune.forget_wisdom()
+    if args.wisdom:
+        with open(args.wisdom) as f:
+            tune.import_wisdom(f.read())
+        wisdom32 = json.loads(tune.export_wisdom())
+    else:
+        tune.autotune("r2c", "f64", [ROWS, COLS], batch=B)
+        wisdom32 = tune.autotune("r2c", "f32mixed", [ROWS, COLS], batch=B)
+    if args.save_wisdom and rank == 0:
+        with open(args.save_wisdom, "w") as f:
+            f.write(tune.export_wisdom())
+
     # FP64 form: inputs in HBM, 2 x 268 MB per direction > L2
     x64 = torch.from_numpy(gen_images(B, 1 + rank)).cuda().reshape(B, -1)
     p64 = DevicePlan("r2c", "f64", [ROWS, COLS], batch=B)
@@ -330,7 +345,8 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "images_per_step_per_gpu": B, "rows": ROWS, "cols": COLS,
                    "l2": "inputs larger than L2 (%.0f MB per direction per GPU)" % (B * ROWS * COLS * 8 / 1e6),
-                   "parallelism": "replicas" if world == 1 else "batch-sharded x%d" % world},
+                   "parallelism": "replicas" if world == 1 else "batch-sharded x%d" % world,
+                   "autotuned": {"schedule": wisdom32["schedule"], "lpc": wisdom32["lpc"]}},
         "transforms_per_s": round(world * args.steps * B * 2 / t64, 1),
         "hbm_frac": round(gbs64 / world / peak, 4),
         "rel_l2_f64_vs_oracle": rel64, "roundtrip_max_abs_f64": rt64,
@@ -358,10 +374,12 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--batch", type=int, default=32, help="images per step per GPU")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--wisdom", default=None, help="import tuning settings instead of autotuning")
+    ap.add_argument("--save-wisdom", default=None, help="write the tuning settings used")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

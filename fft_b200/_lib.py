@@ -84,6 +84,11 @@ SIGNATURES = {
     "gofft_set_pipelined": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int]),
     "gofft_set_schedule": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int]),
     "gofft_get_schedule": (ctypes.c_int, [ctypes.c_int, _i64]),
+    "gofft_autotune": (_i64, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _i64, ctypes.c_char_p, _i64]),
+    "gofft_autotune_uneven": (_i64, [ctypes.c_int, _vp, _i64, ctypes.c_char_p, _i64]),
+    "gofft_wisdom_export": (_i64, [ctypes.c_char_p, _i64]),
+    "gofft_wisdom_import": (ctypes.c_int, [ctypes.c_char_p]),
+    "gofft_wisdom_forget": (ctypes.c_int, []),
 }
 
 _lib = None

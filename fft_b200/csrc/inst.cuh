@@ -35,7 +35,9 @@ template <class P, int M, int GROUP> KFn pick_line(int op) {
 // FP64 lines use 16 register elements per thread (32 would spill); the FP32
 // forms also get a 32-element variant for lines longer than 16 x 512.
 template <class P, int GROUP> KFn pick_maxe(int maxe, int op) {
-  if (maxe == 16) return pick_line<P, 16, GROUP>(op);
+  // 8-element schedules run in the 16-element kernel (the second register
+  // half stays unused)
+  if (maxe <= 16) return pick_line<P, 16, GROUP>(op);
   if constexpr (sizeof(typename P::cpx) == 8) {
     if (maxe == 32) return pick_line<P, 32, GROUP>(op);
   }

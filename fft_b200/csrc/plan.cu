@@ -127,6 +127,12 @@ int get_sched_variant(int prec, long long n) {
   return it == g_sched.end() ? 0 : it->second;
 }
 int sched_epoch() { return g_sched_epoch.load(); }
+std::vector<std::array<long long, 3>> list_sched_variants() {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  std::vector<std::array<long long, 3>> v;
+  for (auto &kv : g_sched) v.push_back({kv.first.first, kv.first.second, kv.second});
+  return v;
+}
 
 // Radix schedule of a 13-smooth length for the Stockham stages: the power of
 // two is split into as few stages of radix at most 2^maxlog as possible with
@@ -438,6 +444,31 @@ void set_lpc_override(int prec, long long n, int op, int colmode, int lpc) {
   std::lock_guard<std::mutex> lk(g_lpc_mu);
   if (lpc <= 0) g_lpc.erase(std::make_tuple(prec, n, op, colmode));
   else g_lpc[std::make_tuple(prec, n, op, colmode)] = lpc;
+}
+std::vector<std::array<long long, 5>> list_lpc_overrides() {
+  std::lock_guard<std::mutex> lk(g_lpc_mu);
+  std::vector<std::array<long long, 5>> v;
+  for (auto &kv : g_lpc)
+    v.push_back({std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first), std::get<3>(kv.first),
+                 kv.second});
+  return v;
+}
+std::vector<std::array<long long, 4>> list_pipe_overrides() {
+  std::lock_guard<std::mutex> lk(g_lpc_mu);
+  std::vector<std::array<long long, 4>> v;
+  for (auto &kv : g_pipe)
+    if (kv.second) v.push_back({std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first), kv.second});
+  return v;
+}
+void clear_overrides() {
+  {
+    std::lock_guard<std::mutex> lk(g_lpc_mu);
+    g_lpc.clear();
+    g_pipe.clear();
+  }
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  g_sched.clear();
+  g_sched_epoch.fetch_add(1);
 }
 int get_lpc_override(int prec, long long n, int op, int colmode) {
   std::lock_guard<std::mutex> lk(g_lpc_mu);

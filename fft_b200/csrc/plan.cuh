@@ -16,6 +16,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -47,6 +48,11 @@ std::vector<int> gpu_radices(long long n, int maxlog = 4);
 void set_sched_variant(int prec, long long n, int v);
 int get_sched_variant(int prec, long long n);
 int sched_epoch();
+// The tuning overrides as lists (for wisdom export) and a reset.
+std::vector<std::array<long long, 3>> list_sched_variants();        // prec, n, variant
+std::vector<std::array<long long, 5>> list_lpc_overrides();         // prec, n, op, colmode, lpc
+std::vector<std::array<long long, 4>> list_pipe_overrides();        // prec, n, op, on
+void clear_overrides();
 
 struct DevProg {
   int n = 0, prec = 0, maxe = 16, device = 0;

@@ -3,6 +3,7 @@
     python -m fft_b200.prof rfft2 --prec f64 --batch 16 --reps 3
     python -m fft_b200.prof c2c --n 1024 --prec f64 --batch 4096 --reps 3
     python -m fft_b200.prof fftn --shape 256,256,256 --prec f32mixed
+    python -m fft_b200.prof rfft2 --prec f64 --wisdom wisdom.json
 
 Prints the CUDA-event time per repetition (taken without a profiler; under a
 profiler the printed times are not measurements).
@@ -23,8 +24,13 @@ def main():
     ap.add_argument("--shape", default="1024,1024")
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--wisdom", default=None, help="tuning settings (JSON) to import first")
     a = ap.parse_args()
     torch.cuda.set_device(0)
+    if a.wisdom:
+        from .tune import import_wisdom
+        with open(a.wisdom) as f:
+            import_wisdom(f.read())
     g = np.random.default_rng(0)
     rdt = torch.float64 if a.prec == "f64" else torch.float32
     cdt = torch.complex128 if a.prec == "f64" else torch.complex64

@@ -294,6 +294,30 @@ GOFFT_API int gofft_set_pipelined(int precision, int64_t n, int op, int on);
 GOFFT_API int gofft_set_schedule(int precision, int64_t n, int variant);
 GOFFT_API int gofft_get_schedule(int precision, int64_t n);
 
+/* Autotuner (no counterpart in the reference, whose plans are fixed by
+ * plan.go's router).  Times candidate settings for batch transforms of
+ * `shape` on the current device -- the radix-schedule variant of each line
+ * length, then the lines per CTA of each pass -- keeps the fastest, and
+ * leaves them set for plans created afterwards (process-wide per precision
+ * and length, like FFTW wisdom).  Allocates its own buffers; takes one forward
+ * and inverse transform per candidate.  Writes the resulting wisdom (JSON)
+ * to `wisdom` (at most cap bytes, may be NULL) and returns its full length,
+ * or minus a status on error. */
+GOFFT_API int64_t gofft_autotune(int kind, int precision, const int64_t *shape, int rank, int64_t batch,
+                                 char *wisdom, int64_t cap);
+/* The same for an uneven batch (gofft_uneven_create's lengths): the schedule
+ * variant of each length class. */
+GOFFT_API int64_t gofft_autotune_uneven(int precision, const int64_t *lengths, int64_t count, char *wisdom,
+                                        int64_t cap);
+/* Current wisdom as JSON: {"gofft_wisdom":1,"schedule":[[prec,n,variant],..],
+ * "lpc":[[prec,n,op,colmode,lpc],..],"pipe":[[prec,n,op,on],..]}. */
+GOFFT_API int64_t gofft_wisdom_export(char *buf, int64_t cap);
+/* Applies exported wisdom (entries are added to / replace the current
+ * settings); GOFFT_EINVAL on a malformed document, nothing applied then. */
+GOFFT_API int gofft_wisdom_import(const char *json);
+/* Drops all tuning settings (defaults again for plans created afterwards). */
+GOFFT_API int gofft_wisdom_forget(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -94,3 +94,25 @@ def test_host_only_edge_cases():
     assert G.Hann(0).size == 0 and list(G.Hann(1)) == [1]
     sc = G.FFTN(np.array([3 - 2j]), [])
     assert sc.size == 1 and sc[0] == 3 - 2j
+
+
+def test_wisdom_roundtrip():
+    """Wisdom import/export is host logic: entries set, listed and cleared."""
+    import json
+    from fft_b200 import tune
+    from fft_b200._lib import GoFFTError, lib
+    tune.forget_wisdom()
+    w = {"gofft_wisdom": 1, "schedule": [[0, 512, 1], [2, 1024, 1]], "lpc": [[0, 1024, 0, 1, 8]],
+         "pipe": [[1, 256, 0, 1]]}
+    tune.import_wisdom(w)
+    got = json.loads(tune.export_wisdom())
+    assert sorted(got["schedule"]) == sorted(w["schedule"])
+    assert got["lpc"] == w["lpc"] and got["pipe"] == w["pipe"]
+    assert lib().gofft_get_schedule(0, 512) == 1 and lib().gofft_get_schedule(0, 1024) == 0
+    for bad in ['{"schedule": [[0, 512, 1]]}', '{"gofft_wisdom":1,"schedule":[[0,512]]}',
+                '{"gofft_wisdom":1,"schedule":[[0,512,7]]}', '{"gofft_wisdom":1,"lpc":[[0,1,99,0,4]]}']:
+        with pytest.raises(GoFFTError):
+            tune.import_wisdom(bad)
+    tune.forget_wisdom()
+    got = json.loads(tune.export_wisdom())
+    assert got["schedule"] == [] and got["lpc"] == [] and got["pipe"] == []
