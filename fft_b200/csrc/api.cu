@@ -822,7 +822,7 @@ extern "C" int gofft_set_pipelined(int precision, int64_t n, int op, int on) {
 }
 
 extern "C" int gofft_set_schedule(int precision, int64_t n, int variant) {
-  if (precision < 0 || precision > 2 || n < 1 || variant < 0 || variant > 1)
+  if (precision < 0 || precision > 2 || n < 1 || variant < 0 || variant > 2)
     return set_err(GOFFT_EINVAL, "bad schedule override");
   set_sched_variant(precision, n, variant);
   return GOFFT_OK;

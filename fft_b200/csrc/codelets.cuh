@@ -4,8 +4,8 @@
 // array of R complex values.  The inverse transform is never coded separately:
 // the engine conjugates on load and on store (IDFT(x) = conj(DFT(conj(x)))).
 //
-// Radix 2/4/8/16 are the power-of-two building blocks (16 = 4 x 4 with the
-// W16 twiddles as constants); odd primes R in {3,5,7,11,13} share one
+// Radix 2/4/8/16/32 are the power-of-two building blocks (16 = 4 x 4 and
+// 32 = 4 x 8 with their twiddles as constants); odd primes R in {3,5,7,11,13} share one
 // conjugate-pair template: with s_q = v_q + v_{R-q}, d_q = v_q - v_{R-q},
 //   X[k]   = v0 + sum_q cos(2 pi q k / R) s_q - i sum_q sin(2 pi q k / R) d_q
 //   X[R-k] = v0 + sum_q cos(2 pi q k / R) s_q + i sum_q sin(2 pi q k / R) d_q
@@ -140,6 +140,69 @@ template <class C> struct Dft<16, C> {
       C a = y[k2], b = y[4 + k2], c = y[8 + k2], d = y[12 + k2];
       dft4(a, b, c, d);
       v[k2] = a; v[k2 + 4] = b; v[k2 + 8] = c; v[k2 + 12] = d;
+    }
+  }
+};
+
+// cos(pi e / 16) and sin(pi e / 16) for any integer e (the W32 constants).
+GF_HD constexpr double cos16(int e) {
+  constexpr double t[9] = {1.0,
+                           0.9807852804032304491261822,
+                           0.9238795325112867561281832,
+                           0.8314696123025452370787884,
+                           0.7071067811865475244008444,
+                           0.5555702330196022247428308,
+                           0.3826834323650897717284600,
+                           0.1950903220161282678482849,
+                           0.0};
+  return ((e % 32) + 32) % 32 <= 8    ? t[((e % 32) + 32) % 32]
+         : ((e % 32) + 32) % 32 <= 16 ? -t[16 - ((e % 32) + 32) % 32]
+         : ((e % 32) + 32) % 32 <= 24 ? -t[((e % 32) + 32) % 32 - 16]
+                                      : t[32 - ((e % 32) + 32) % 32];
+}
+GF_HD constexpr double sin16(int e) { return cos16(8 - e); }
+
+// z * W32^e = z * exp(-2 pi i e / 32), with the trivial angles folded.
+template <int E, class C> GF_DEV C tw32(C z) {
+  using Rl = decltype(z.x);
+  constexpr int e = ((E % 32) + 32) % 32;
+  if constexpr (e == 0) return z;
+  else if constexpr (e == 8) return cmul_mi(z);
+  else if constexpr (e == 16) return mkc(-z.x, -z.y);
+  else if constexpr (e == 24) return cmul_pi(z);
+  else if constexpr (e == 4) return mul_w8_1(z);
+  else if constexpr (e == 12) return mul_w8_3(z);
+  else return cmul(z, mkc((Rl)cos16(e), (Rl)-sin16(e)));
+}
+
+// DFT-32 as 4 x 8: n = n1 + 4 n2, k = k2 + 8 k1; DFT-8 over n2 for each n1,
+// twiddles W32^(n1 k2), DFT-4 over n1 for each k2.
+template <int N1, class C> GF_DEV void dft32_col(C *v, C (&y)[32]) {
+  C t[8];
+#pragma unroll
+  for (int n2 = 0; n2 < 8; n2++) t[n2] = v[N1 + 4 * n2];
+  Dft<8, C>::run(t);
+  y[N1 * 8 + 0] = t[0];
+  y[N1 * 8 + 1] = tw32<N1 * 1>(t[1]);
+  y[N1 * 8 + 2] = tw32<N1 * 2>(t[2]);
+  y[N1 * 8 + 3] = tw32<N1 * 3>(t[3]);
+  y[N1 * 8 + 4] = tw32<N1 * 4>(t[4]);
+  y[N1 * 8 + 5] = tw32<N1 * 5>(t[5]);
+  y[N1 * 8 + 6] = tw32<N1 * 6>(t[6]);
+  y[N1 * 8 + 7] = tw32<N1 * 7>(t[7]);
+}
+template <class C> struct Dft<32, C> {
+  static GF_DEV void run(C *v) {
+    C y[32];
+    dft32_col<0>(v, y);
+    dft32_col<1>(v, y);
+    dft32_col<2>(v, y);
+    dft32_col<3>(v, y);
+#pragma unroll
+    for (int k2 = 0; k2 < 8; k2++) {
+      C a = y[k2], b = y[8 + k2], c = y[16 + k2], d = y[24 + k2];
+      dft4(a, b, c, d);
+      v[k2] = a; v[k2 + 8] = b; v[k2 + 16] = c; v[k2 + 24] = d;
     }
   }
 };

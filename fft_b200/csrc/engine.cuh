@@ -225,6 +225,9 @@ GF_DEV void stage_sw(int R, typename P::cpx (&v)[MAXE], const LineView<typename 
     case 11: stage<P, Op, 11, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
     case 13: stage<P, Op, 13, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
     case 16: stage<P, Op, 16, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj); break;
+    case 32:
+      if constexpr (MAXE >= 32) stage<P, Op, 32, MAXE, FG, TG>(v, s, a, c, ns, nsd, tw, cj);
+      break;
     default: break;
   }
 }
@@ -291,24 +294,56 @@ GF_DEV void run_stages(const LineView<typename P::cpx> &s, const KArgs &a, const
 template <class F>
 GF_DEV void tile_loop(const Side &sd, int lpc, int len, FastDiv ldiv, FastDiv lpcdiv,
                       long long line0, long long nlines, F f) {
-  const int total = lpc * len;
-  if (sd.stride == 1 || lpc == 1) {
+  const int tl = (int)lpcdiv.div((uint32_t)blockDim.x);  // threads per line here
+  if ((sd.stride == 1 || lpc == 1) && tl < 8) {
+    // short lines: walk the tile element by element so a warp spans lines
+    const int total = lpc * len;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       uint32_t l, i;
       ldiv.divmod((uint32_t)e, l, i);
       const long long gl = line0 + l;
       if (gl < nlines) f((int)l, (int)i, line_off(sd, (uint32_t)gl) + (long long)i * sd.stride);
     }
-  } else {
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      uint32_t i, l;
-      lpcdiv.divmod((uint32_t)e, i, l);
-      const long long gl = line0 + l;
-      if (gl < nlines) f((int)l, (int)i, line_off(sd, (uint32_t)gl) + (long long)i * sd.stride);
-    }
+    return;
   }
+  // each thread keeps one line: its offset is computed once, the elements
+  // step by the threads per line (along the line in row mode, so a warp
+  // reads one contiguous run; across lines in column mode, so consecutive
+  // threads touch consecutive lines)
+  if ((int)threadIdx.x >= tl * lpc) return;
+  uint32_t l, i0;
+  if (sd.stride == 1 || lpc == 1) {
+    l = threadIdx.x / (uint32_t)tl;
+    i0 = threadIdx.x - l * (uint32_t)tl;
+  } else {
+    lpcdiv.divmod(threadIdx.x, i0, l);
+  }
+  const long long gl = line0 + l;
+  if (gl >= nlines) return;
+  const long long st = sd.stride;
+  long long off = line_off(sd, (uint32_t)gl) + (long long)i0 * st;
+  const long long dst = (long long)tl * st;
+  for (int i = (int)i0; i < len; i += tl, off += dst) f((int)l, i, off);
 }
 
+// A loop over the tile's elements in shared memory only (no global side):
+// every (line, element) pair once, each thread on one line, consecutive
+// threads on consecutive elements (row layout) or consecutive lines (column
+// layout) so shared-memory accesses stay conflict-free.
+template <class F>
+GF_DEV void smem_loop(const KArgs &a, int len, F f) {
+  const int lpc = a.lpc;
+  const int tl = (int)a.lpcdiv.div((uint32_t)blockDim.x);
+  if ((int)threadIdx.x >= tl * lpc) return;
+  uint32_t l, i0;
+  if (a.flags & GF_COLMAP) {
+    a.lpcdiv.divmod(threadIdx.x, i0, l);
+  } else {
+    l = threadIdx.x / (uint32_t)tl;
+    i0 = threadIdx.x - l * (uint32_t)tl;
+  }
+  for (int i = (int)i0; i < len; i += tl) f((int)l, i);
+}
 
 // ---------------------------------------------------------------------------
 // Compile-time schedules.  For the hot lengths the radix list, the threads

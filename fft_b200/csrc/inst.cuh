@@ -48,8 +48,9 @@ template <class P, int GROUP> KFn pick_maxe(int maxe, int op) {
 // radices...).  Each length has the run-time heuristic's lines per CTA and
 // twice that (column transforms of FP32 data); the schedules are those
 // gpu_radices() and pick_threads() derive for the length, the default
-// variant first, then the radix-8 variant (8 elements per thread) for the
-// lengths of the 2-D workloads.
+// variant first, then the radix-8 variant (8 elements per thread) and the
+// FP32 radix-32 variant (32 elements per thread) for the lengths of the 2-D
+// workloads.
 #define GF_CT_LIST(X)                                                     \
   X(64, 4, 64, 1, 8, 8) X(64, 4, 128, 0, 8, 8)                           \
   X(128, 8, 32, 1, 16, 8) X(128, 8, 64, 0, 16, 8)                        \
@@ -63,7 +64,8 @@ template <class P, int GROUP> KFn pick_maxe(int maxe, int op) {
   X(256, 32, 8, 1, 8, 8, 4) X(256, 32, 16, 0, 8, 8, 4)                   \
   X(512, 64, 4, 1, 8, 8, 8) X(512, 64, 8, 0, 8, 8, 8)                    \
   X(1024, 128, 2, 1, 8, 8, 4, 4) X(1024, 128, 4, 0, 8, 8, 4, 4)          \
-  X(2048, 256, 1, 1, 8, 8, 8, 4) X(2048, 256, 2, 0, 8, 8, 8, 4)
+  X(2048, 256, 1, 1, 8, 8, 8, 4) X(2048, 256, 2, 0, 8, 8, 8, 4)          \
+  X(512, 16, 16, 1, 32, 16) X(1024, 32, 8, 1, 32, 32)
 
 template <int... Rs> constexpr bool sched_eq(const int *r, int nst) {
   constexpr int a[] = {Rs...};
@@ -84,11 +86,15 @@ template <class P, int GROUP, int N, int T, int L, bool ROWOPS, int... Rs> KFn c
   // FP64 radix-16 butterflies need ~128 registers (two 256-thread CTAs per
   // SM); the FP32 forms and the 8-element schedules fit in fewer, so ask for
   // more resident CTAs (more warps to hide shared-memory and twiddle
-  // latency): 8-element schedules get 64 registers a thread.
+  // latency): 8-element schedules get 64 registers a thread, 32-element
+  // (FP32) ones 128.
   constexpr int E = ct_maxe_r<N, T, Rs...>();
-  constexpr int MINB = (E <= 8) ? (65536 / (L * T * 64) > 0 ? 65536 / (L * T * 64) : 1)
-                                : (L * T <= 256) ? (sizeof(typename P::cpx) == 16 ? 2 : GF_F32_MINB) : 1;
-  if constexpr (N == 16384 && sizeof(typename P::cpx) == 16) {
+  constexpr int MINB = (E <= 8)    ? (65536 / (L * T * 64) > 0 ? 65536 / (L * T * 64) : 1)
+                       : (E >= 32) ? (65536 / (L * T * 128) > 0 ? 65536 / (L * T * 128) : 1)
+                       : (L * T <= 256) ? (sizeof(typename P::cpx) == 16 ? 2 : GF_F32_MINB) : 1;
+  if constexpr (sizeof(typename P::cpx) == 16 && E > 16) {
+    return nullptr;  // 32-element FP64 schedules would spill; not built
+  } else if constexpr (N == 16384 && sizeof(typename P::cpx) == 16) {
     return nullptr;  // FP64 16384 is two-pass
   } else if constexpr (GROUP == 0) {
     switch (op) {

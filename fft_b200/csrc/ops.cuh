@@ -235,16 +235,14 @@ struct OpC2RPacked {
     const int m = a.lp.n;
     const int h = m / 2 + 1;
     const Rl half = (Rl)0.5;
-    const int total = a.lpc * h;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int l = e / h, k = e - l * h;
-      if (line0 + l >= a.nlines) continue;
+    smem_loop(a, h, [&](int l, int k) {
+      if (line0 + l >= a.nlines) return;
       const LineView<C> s = line_view<C>(a, l, sb);
       if (k == 0) {
         const Rl x0 = s[0].x, xm = s[m].x;
         // Z[0] = ((x0+xm) + i(x0-xm))/2, stored conjugated
         s[0] = mkc((x0 + xm) * half, -(x0 - xm) * half);
-        continue;
+        return;
       }
       C xk = s[k], xmk = s[m - k];
       if (a.ic & GF_EDGE_WEIGHT) {  // interior bins enter halved (k = m/2 too)
@@ -258,7 +256,7 @@ struct OpC2RPacked {
       // Z[k] = xe + i xo ; Z[m-k] = conj(xe - i xo); stored conjugated
       s[k] = cconj(mkc(xe.x - xo.y, xe.y + xo.x));
       if (m - k != k) s[m - k] = cconj(mkc(xe.x + xo.y, -(xe.y - xo.x)));
-    }
+    });
     __syncthreads();
   }
   template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
@@ -337,25 +335,23 @@ struct OpC2RFull {
     const int h = n / 2 + 1;
     const int up = n - h;  // mirrored elements i = h .. n-1
     if (a.ic & GF_EDGE_WEIGHT) {
-      for (int e = threadIdx.x; e < a.lpc * h; e += blockDim.x) {
-        const int l = e / h, i = e - l * h;
-        if (i == 0 || 2 * i == n) continue;
+      smem_loop(a, h, [&](int l, int i) {
+        if (i == 0 || 2 * i == n) return;
         const LineView<C> s = line_view<C>(a, l, sb);
         s[i] = mkc(s[i].x * (typename P::real)0.5, s[i].y * (typename P::real)0.5);
-      }
+      });
       __syncthreads();
     }
-    for (int e = threadIdx.x; e < a.lpc * up; e += blockDim.x) {
-      const int l = e / up, i = h + (e - l * up);
+    smem_loop(a, up, [&](int l, int e) {
+      const int i = h + e;
       const LineView<C> s = line_view<C>(a, l, sb);
       s[i] = s[n - i];  // conj(conj(bin(n-i)))
-    }
+    });
     __syncthreads();
-    for (int e = threadIdx.x; e < a.lpc * h; e += blockDim.x) {
-      const int l = e / h, i = e - l * h;
+    smem_loop(a, h, [&](int l, int i) {
       const LineView<C> s = line_view<C>(a, l, sb);
       s[i].y = -s[i].y;
-    }
+    });
     __syncthreads();
   }
   template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
@@ -526,26 +522,22 @@ struct OpBluestein {
     using SP = typename P::sp_t;
     const SP *w = (const SP *)a.aux0;
     const int n = (int)a.ia;
-    for (int e = threadIdx.x; e < a.lpc * n; e += blockDim.x) {
-      const int l = e / n, j = e - l * n;
+    smem_loop(a, n, [&](int l, int j) {
       const LineView<C> s = line_view<C>(a, l, sb);
       C v = s[j];
       if (a.cj_in) v.y = -v.y;
       s[j] = spmul(v, __ldg(&w[j]));
-    }
+    });
     __syncthreads();
   }
   template <class P> static GF_DEV void mid(const KArgs &a, long long, bool, void *sb = nullptr) {
     using C = Cx<P>;
     using SP = typename P::sp_t;
     const SP *B = (const SP *)a.aux2;
-    const int total = a.lpc * a.lp.n;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      uint32_t l, k;
-      a.ndiv.divmod((uint32_t)e, l, k);
-      const LineView<C> s = line_view<C>(a, (int)l, sb);
+    smem_loop(a, a.lp.n, [&](int l, int k) {
+      const LineView<C> s = line_view<C>(a, l, sb);
       s[k] = cconj(spmul(s[k], __ldg(&B[k])));
-    }
+    });
     __syncthreads();
   }
   template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {
@@ -596,12 +588,11 @@ struct OpSpectro {
     using Rl = typename P::real;
     const Rl *win = (const Rl *)a.aux1;
     const int m = a.lp.n;
-    for (int e = threadIdx.x; e < a.lpc * m; e += blockDim.x) {
-      const int l = e / m, j = e - l * m;
+    smem_loop(a, m, [&](int l, int j) {
       const LineView<C> s = line_view<C>(a, l, sb);
       C v = s[j];
       s[j] = mkc(v.x * __ldg(&win[2 * j]), v.y * __ldg(&win[2 * j + 1]));
-    }
+    });
     __syncthreads();
   }
   template <class P> static GF_DEV void store(const KArgs &a, long long line0, void *sb = nullptr) {

@@ -109,7 +109,9 @@ long long best_conv_len(long long lo) {
 // Schedule variants per (precision, length): 0 = radices up to 16 with 16
 // (FP64) or up to 32 (FP32) elements per thread; 1 = radices up to 8 with 8
 // elements per thread (twice the threads per line, about half the registers,
-// more resident warps, one more stage).  Objects built under one setting are
+// more resident warps, one more stage); 2 (FP32 forms) = radices up to 32
+// with 32 elements per thread (fewer stages: fewer barriers, shared-memory
+// exchanges and twiddle loads, more registers).  Objects built under one setting are
 // cached apart from those built under another (the epoch is part of every
 // cache key).
 static std::mutex g_sched_mu;
@@ -248,11 +250,21 @@ static bool schedule_for(long long n, int prec, int &maxe, int &T, std::vector<i
   if (n < 1 || !smooth13(n)) return false;
   const size_t bytes = (size_t)spad_size((int)n) * csize(prec) + 2 * csize(prec);
   if (bytes > max_smem_optin()) return false;
-  if (get_sched_variant(prec, n) == 1) {
+  const int var = get_sched_variant(prec, n);
+  if (var == 1) {
     rad = gpu_radices(n, 3);
     const int t = (int)rad.size() <= GF_MAXST ? pick_threads(n, 8, rad) : -1;
     if (t > 0) {
       maxe = 8;
+      T = t;
+      return true;
+    }
+  }
+  if (var == 2 && prec != F64) {
+    rad = gpu_radices(n, 5);
+    const int t = (int)rad.size() <= GF_MAXST ? pick_threads(n, 32, rad) : -1;
+    if (t > 0) {
+      maxe = 32;
       T = t;
       return true;
     }

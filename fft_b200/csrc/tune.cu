@@ -247,15 +247,21 @@ extern "C" int64_t gofft_autotune(int kind, int precision, const int64_t *shape,
   double best = 0;
   rc = time_plan(kind, precision, sh, batch, s, &best);
   // 1. schedule variants: coordinate descent over the distinct lengths
+  const int nvar = precision == GOFFT_F64 ? 2 : 3;
   for (size_t li = 0; li < lens.size() && !rc; li++) {
     const long long n = lens[li];
-    const int cur = get_sched_variant(precision, n);
-    set_sched_variant(precision, n, 1 - cur);
-    double t = 0;
-    if (time_plan(kind, precision, sh, batch, s, &t) == 0 && t < best * 0.98) {
-      best = t;
-    } else {
-      set_sched_variant(precision, n, cur);
+    int keep = get_sched_variant(precision, n);
+    for (int v = 0; v < nvar; v++) {
+      if (v == keep) continue;
+      const int prev = keep;
+      set_sched_variant(precision, n, v);
+      double t = 0;
+      if (time_plan(kind, precision, sh, batch, s, &t) == 0 && t < best * 0.98) {
+        best = t;
+        keep = v;
+      } else {
+        set_sched_variant(precision, n, prev);
+      }
     }
   }
   // 2. lines per CTA of each pass (the kernels pick it at launch)
@@ -321,13 +327,22 @@ extern "C" int64_t gofft_autotune_uneven(int precision, const int64_t *lengths, 
   };
   double best = 0;
   if (!rc) rc = measure(&best);
+  const int nvar = precision == GOFFT_F64 ? 2 : 3;
   for (long long n : cls) {
     if (rc) break;
-    const int cur = get_sched_variant(precision, n);
-    set_sched_variant(precision, n, 1 - cur);
-    double t = 0;
-    if (measure(&t) == 0 && t < best * 0.98) best = t;
-    else set_sched_variant(precision, n, cur);
+    int keep = get_sched_variant(precision, n);
+    for (int v = 0; v < nvar; v++) {
+      if (v == keep) continue;
+      const int prev = keep;
+      set_sched_variant(precision, n, v);
+      double t = 0;
+      if (measure(&t) == 0 && t < best * 0.98) {
+        best = t;
+        keep = v;
+      } else {
+        set_sched_variant(precision, n, prev);
+      }
+    }
   }
   cudaStreamDestroy(s);
   if (rc) return -rc;
@@ -344,7 +359,7 @@ extern "C" int gofft_wisdom_import(const char *json) {
   if (!parse_tuples(js, "schedule", 3, sc) || !parse_tuples(js, "lpc", 5, lp) || !parse_tuples(js, "pipe", 4, pp))
     return set_err(GOFFT_EINVAL, "malformed wisdom");
   for (auto &t : sc)
-    if (t[0] < 0 || t[0] > 2 || t[1] < 1 || t[2] < 0 || t[2] > 1) return set_err(GOFFT_EINVAL, "bad schedule entry");
+    if (t[0] < 0 || t[0] > 2 || t[1] < 1 || t[2] < 0 || t[2] > 2) return set_err(GOFFT_EINVAL, "bad schedule entry");
   for (auto &t : lp)
     if (t[0] < 0 || t[0] > 2 || t[1] < 1 || t[2] < 0 || t[2] >= OP_COUNT || t[4] < 0 || t[4] > 512)
       return set_err(GOFFT_EINVAL, "bad lpc entry");

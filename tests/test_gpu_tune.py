@@ -1,4 +1,4 @@
-"""The autotuner and the radix-8 schedule variant: tuned and varied plans
+"""The autotuner and the radix-8 / radix-32 schedule variants: tuned and varied plans
 still match the oracle (settings are process-wide, so every test here puts
 the defaults back)."""
 import numpy as np
@@ -22,13 +22,14 @@ def defaults():
     tune.forget_wisdom()
 
 
+@pytest.mark.parametrize("var", [1, 2])
 @pytest.mark.parametrize("prec", ["f64", "f32mixed", "f32"])
 @pytest.mark.parametrize("n", [8, 64, 128, 256, 512, 1024, 2048, 4096, 360, 1000, 1009, 10007, 65536])
-def test_variant1_c2c(prec, n):
+def test_variant_c2c(var, prec, n):
     from fft_b200._lib import lib
     from fft_b200.device import DevicePlan
-    for m in {n, 1008}:
-        lib().gofft_set_schedule(PREC[prec], m, 1)
+    for m in {n, 1008, 256}:
+        lib().gofft_set_schedule(PREC[prec], m, var)
     B = 5
     g = rng(n)
     x = g.standard_normal((B, n)) + 1j * g.standard_normal((B, n))
@@ -39,14 +40,15 @@ def test_variant1_c2c(prec, n):
     assert rel_l2(p.c2c(xt, inverse=True).cpu().numpy(), O.batch_fft(x, inverse=True)) <= TOL[prec]
 
 
-@pytest.mark.parametrize("prec", ["f64", "f32mixed"])
+@pytest.mark.parametrize("var", [1, 2])
+@pytest.mark.parametrize("prec", ["f64", "f32mixed", "f32"])
 @pytest.mark.parametrize("shape", [[1024, 1024], [512, 512], [256, 512], [64, 2048], [30, 1000]])
-def test_variant1_rfft2(prec, shape):
+def test_variant_rfft2(var, prec, shape):
     from fft_b200._lib import lib
     from fft_b200.device import DevicePlan
     R, C = shape
     for m in {R, C // 2}:
-        lib().gofft_set_schedule(PREC[prec], m, 1)
+        lib().gofft_set_schedule(PREC[prec], m, var)
     B = 3
     x = rng(R + C).standard_normal((B, R, C))
     rdt = torch.float64 if prec == "f64" else torch.float32
