@@ -366,9 +366,16 @@ template <int N, int T, int R, int... Rs> constexpr int ct_maxe_r() {
   }
 }
 
-template <class P, class Op, int N, int T, int NS, int R, int E, bool FG, bool TG>
-GF_DEV void stage_ct(typename P::cpx (&v)[E], const LineView<typename P::cpx> &s, const KArgs &a,
-                     const LineCtx &c, const typename P::tw_t *tw, bool cj) {
+// Shared-memory slot of element i of a line at base b with element step STEP
+// (1 in row layout, the lines per CTA in column layout).  For index runs
+// i + r*D with D a multiple of 16 the padded slots are spad(i) + r*(D + D/16),
+// so a butterfly's loads and stores share one base address and immediate
+// offsets.
+template <int STEP, class C> GF_DEV C &slot(C *b, int i) { return b[spad(i) * STEP]; }
+
+template <class P, class Op, int N, int T, int NS, int R, int E, bool FG, bool TG, int STEP>
+GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &a, const LineCtx &c,
+                     const typename P::tw_t *tw, bool cj) {
   using C = typename P::cpx;
   constexpr int NB = N / R;
   constexpr int PER = (NB + T - 1) / T;
@@ -377,13 +384,23 @@ GF_DEV void stage_ct(typename P::cpx (&v)[E], const LineView<typename P::cpx> &s
   for (int b = 0; b < PER; b++) {
     const int j = c.t + b * T;
     if (EXACT || j < NB) {
+      if constexpr (!FG && NB % 16 == 0) {
+        const C *p = &slot<STEP>(sb, j);
 #pragma unroll
-      for (int r = 0; r < R; r++) {
-        C x;
-        if constexpr (FG) x = Op::template gload<P>(a, c, j + r * NB);
-        else x = s[j + r * NB];
-        if (cj) x.y = -x.y;
-        v[b * R + r] = x;
+        for (int r = 0; r < R; r++) {
+          C x = p[r * (NB + NB / 16) * STEP];
+          if (cj) x.y = -x.y;
+          v[b * R + r] = x;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          C x;
+          if constexpr (FG) x = Op::template gload<P>(a, c, j + r * NB);
+          else x = slot<STEP>(sb, j + r * NB);
+          if (cj) x.y = -x.y;
+          v[b * R + r] = x;
+        }
       }
     }
   }
@@ -400,20 +417,26 @@ GF_DEV void stage_ct(typename P::cpx (&v)[E], const LineView<typename P::cpx> &s
       }
       Dft<R, C>::run(&v[b * R]);
       const int base = q * NS * R + k;
+      if constexpr (TG) {
 #pragma unroll
-      for (int r = 0; r < R; r++) {
-        if constexpr (TG) Op::template gstore<P>(a, c, base + r * NS, v[b * R + r]);
-        else s[base + r * NS] = v[b * R + r];
+        for (int r = 0; r < R; r++) Op::template gstore<P>(a, c, base + r * NS, v[b * R + r]);
+      } else if constexpr (NS % 16 == 0) {
+        C *p = &slot<STEP>(sb, base);
+#pragma unroll
+        for (int r = 0; r < R; r++) p[r * (NS + NS / 16) * STEP] = v[b * R + r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; r++) slot<STEP>(sb, base + r * NS) = v[b * R + r];
       }
     }
   }
   if constexpr (!TG) __syncthreads();
 }
 
-template <class P, class Op, int N, int T, int NS, int TO, int E, bool CAN_FG, bool CAN_TG, int R,
+template <class P, class Op, int N, int T, int NS, int TO, int E, bool CAN_FG, bool CAN_TG, int STEP, int R,
           int... Rs>
-GF_DEV void stages_ct(typename P::cpx (&v)[E], const LineView<typename P::cpx> &s, const KArgs &a,
-                      const LineCtx &c, bool cj_first, bool fg, bool tg) {
+GF_DEV void stages_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &a, const LineCtx &c,
+                      bool cj_first, bool fg, bool tg) {
   using TW = typename P::tw_t;
   constexpr bool FIRST = NS == 1;
   constexpr bool LAST = sizeof...(Rs) == 0;
@@ -422,29 +445,32 @@ GF_DEV void stages_ct(typename P::cpx (&v)[E], const LineView<typename P::cpx> &
   constexpr bool F_OK = FIRST && CAN_FG;
   constexpr bool T_OK = LAST && CAN_TG;
   if constexpr (F_OK && T_OK) {
-    if (fg && tg) stage_ct<P, Op, N, T, NS, R, E, true, true>(v, s, a, c, tw, cj);
-    else if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false>(v, s, a, c, tw, cj);
-    else if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true>(v, s, a, c, tw, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false>(v, s, a, c, tw, cj);
+    if (fg && tg) stage_ct<P, Op, N, T, NS, R, E, true, true, STEP>(v, sb, a, c, tw, cj);
+    else if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP>(v, sb, a, c, tw, cj);
+    else if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP>(v, sb, a, c, tw, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, cj);
   } else if constexpr (F_OK) {
-    if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false>(v, s, a, c, tw, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false>(v, s, a, c, tw, cj);
+    if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP>(v, sb, a, c, tw, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, cj);
   } else if constexpr (T_OK) {
-    if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true>(v, s, a, c, tw, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false>(v, s, a, c, tw, cj);
+    if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP>(v, sb, a, c, tw, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, cj);
   } else {
-    stage_ct<P, Op, N, T, NS, R, E, false, false>(v, s, a, c, tw, cj);
+    stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, cj);
   }
   if constexpr (!LAST)
-    stages_ct<P, Op, N, T, NS * R, TO + NS * (R - 1), E, CAN_FG, CAN_TG, Rs...>(v, s, a, c, cj_first, fg, tg);
+    stages_ct<P, Op, N, T, NS * R, TO + NS * (R - 1), E, CAN_FG, CAN_TG, STEP, Rs...>(v, sb, a, c, cj_first, fg,
+                                                                                      tg);
 }
 
-template <class P, class Op, int N, int T, bool CAN_FG, bool CAN_TG, int... Rs>
-GF_DEV void run_stages_ct(Sched<Rs...>, const LineView<typename P::cpx> &s, const KArgs &a,
-                          const LineCtx &c, bool cj_first, bool fg, bool tg) {
+// Runs the compiled schedule on the line at shared-memory base sb; STEP is
+// the element step of the layout (1: row layout, LPC: column layout).
+template <class P, class Op, int N, int T, bool CAN_FG, bool CAN_TG, int STEP, int... Rs>
+GF_DEV void run_stages_ct(Sched<Rs...>, typename P::cpx *sb, const KArgs &a, const LineCtx &c, bool cj_first,
+                          bool fg, bool tg) {
   constexpr int E = ct_maxe_r<N, T, Rs...>();
   typename P::cpx v[E];
-  stages_ct<P, Op, N, T, 1, 0, E, CAN_FG, CAN_TG, Rs...>(v, s, a, c, cj_first, fg, tg);
+  stages_ct<P, Op, N, T, 1, 0, E, CAN_FG, CAN_TG, STEP, Rs...>(v, sb, a, c, cj_first, fg, tg);
 }
 
 }  // namespace gf

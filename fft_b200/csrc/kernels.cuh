@@ -172,7 +172,10 @@ __global__ void __launch_bounds__(LPC *T, MINB) k_line_ct(const KArgs a) {
     Op::template prep<P>(a, line0);
   }
   const LineView<C> s = line_view<C>(a, c.l);
-  run_stages_ct<P, Op, N, T, Op::kFG, Op::kTG>(S{}, s, a, c, Op::first_conj(a), first_g, last_g);
+  if (a.flags & GF_COLMAP)
+    run_stages_ct<P, Op, N, T, Op::kFG, Op::kTG, LPC>(S{}, s.b, a, c, Op::first_conj(a), first_g, last_g);
+  else
+    run_stages_ct<P, Op, N, T, Op::kFG, Op::kTG, 1>(S{}, s.b, a, c, Op::first_conj(a), first_g, last_g);
   if (!last_g) Op::template store<P>(a, line0);
 }
 
@@ -225,7 +228,10 @@ __global__ void __launch_bounds__(LPC *T, MINB) k_line_pp(const KArgs a) {
     c.valid = c.line < a.nlines;
     c.ooff = c.valid ? line_off(a.out, (uint32_t)c.line) : 0;
     const LineView<C> s = line_view<C>(a, c.l, bufs[cur]);
-    run_stages_ct<P, Op, N, T, false, Op::kTG>(S{}, s, a, c, Op::first_conj(a), false, last_g);
+    if (a.flags & GF_COLMAP)
+      run_stages_ct<P, Op, N, T, false, Op::kTG, LPC>(S{}, s.b, a, c, Op::first_conj(a), false, last_g);
+    else
+      run_stages_ct<P, Op, N, T, false, Op::kTG, 1>(S{}, s.b, a, c, Op::first_conj(a), false, last_g);
     if (!last_g) Op::template store<P>(a, line0, bufs[cur]);
     __syncthreads();
     cur ^= 1;

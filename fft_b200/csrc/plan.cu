@@ -123,12 +123,19 @@ void set_sched_variant(int prec, long long n, int v) {
   else g_sched[std::make_pair(prec, n)] = v;
   g_sched_epoch.fetch_add(1);
 }
+// Highest variant the calling thread may build (uneven batches run every
+// line in one persistent kernel with 16-element registers, so they cap at 1).
+static thread_local int t_sched_cap = 2;
+SchedCap::SchedCap(int cap) : prev(t_sched_cap) { t_sched_cap = cap; }
+SchedCap::~SchedCap() { t_sched_cap = prev; }
 int get_sched_variant(int prec, long long n) {
   std::lock_guard<std::mutex> lk(g_sched_mu);
   auto it = g_sched.find(std::make_pair(prec, n));
-  return it == g_sched.end() ? 0 : it->second;
+  const int v = it == g_sched.end() ? 0 : it->second;
+  return std::min(v, t_sched_cap);
 }
-int sched_epoch() { return g_sched_epoch.load(); }
+// Cache-key part of the settings: the override epoch and the thread's cap.
+int sched_epoch() { return g_sched_epoch.load() * 4 + t_sched_cap; }
 std::vector<std::array<long long, 3>> list_sched_variants() {
   std::lock_guard<std::mutex> lk(g_sched_mu);
   std::vector<std::array<long long, 3>> v;

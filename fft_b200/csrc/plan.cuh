@@ -48,6 +48,13 @@ std::vector<int> gpu_radices(long long n, int maxlog = 4);
 void set_sched_variant(int prec, long long n, int v);
 int get_sched_variant(int prec, long long n);
 int sched_epoch();
+// Caps the schedule variant for objects the calling thread builds while the
+// guard lives.
+struct SchedCap {
+  int prev;
+  explicit SchedCap(int cap);
+  ~SchedCap();
+};
 // The tuning overrides as lists (for wisdom export) and a reset.
 std::vector<std::array<long long, 3>> list_sched_variants();        // prec, n, variant
 std::vector<std::array<long long, 5>> list_lpc_overrides();         // prec, n, op, colmode, lpc

@@ -327,7 +327,7 @@ extern "C" int64_t gofft_autotune_uneven(int precision, const int64_t *lengths, 
   };
   double best = 0;
   if (!rc) rc = measure(&best);
-  const int nvar = precision == GOFFT_F64 ? 2 : 3;
+  const int nvar = 2;  // uneven batches build variants 0 and 1 only
   for (long long n : cls) {
     if (rc) break;
     int keep = get_sched_variant(precision, n);

@@ -187,6 +187,7 @@ static void rebase_aux(const void *&p, char *ws, size_t wsb) {
 
 extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_t count, const int64_t *in_offsets,
                                    const int64_t *out_offsets, gofft_uneven **out) {
+  SchedCap cap(1);  // every class runs in the persistent kernel's 16-element registers
   if (!out || !lengths || count <= 0) return set_err(GOFFT_EINVAL, "bad uneven batch arguments");
   *out = nullptr;
   if (precision < 0 || precision > 2) return set_err(GOFFT_EINVAL, "bad precision");

@@ -291,8 +291,8 @@ GOFFT_API int gofft_set_pipelined(int precision, int64_t n, int op, int on);
  * 16 elements per thread (FP32: up to 32), the default; 1 = radices up to 8
  * with 8 elements per thread (twice the threads per line, half the
  * registers, one more stage); 2 (FP32 forms only; FP64 keeps 0) = radices up
- * to 32 with 32 elements per thread (fewer stages).  The autotuner's
- * schedule choice. */
+ * to 32 with 32 elements per thread (fewer stages); uneven batches build
+ * at most variant 1.  The autotuner's schedule choice. */
 GOFFT_API int gofft_set_schedule(int precision, int64_t n, int variant);
 GOFFT_API int gofft_get_schedule(int precision, int64_t n);
 

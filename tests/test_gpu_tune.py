@@ -95,3 +95,22 @@ def test_autotune_c2c_and_uneven():
     for part in parts:
         assert rel_l2(got[off:off + part.size], O.fft(part)) <= 1e-6
         off += part.size
+
+
+def test_uneven_caps_variant2():
+    """Uneven batches run every class in the persistent kernel's 16-element
+    registers: a radix-32 setting for one of their lengths is capped, not
+    run wrong."""
+    from fft_b200._lib import lib
+    from fft_b200.device import UnevenBatch
+    lengths = [1024, 512, 4096, 1024, 60]
+    for n in set(lengths):
+        lib().gofft_set_schedule(PREC["f32mixed"], n, 2)
+    parts = [rng(n).standard_normal(n) + 1j * rng(n + 3).standard_normal(n) for n in lengths]
+    u = UnevenBatch("f32mixed", lengths)
+    got = u(torch.from_numpy(np.concatenate(parts).astype(np.complex64)).cuda()).cpu().numpy()
+    assert u.status() == 0
+    off = 0
+    for part in parts:
+        assert rel_l2(got[off:off + part.size], O.fft(part)) <= 1e-6
+        off += part.size
