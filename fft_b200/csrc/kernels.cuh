@@ -142,6 +142,11 @@ __global__ void __launch_bounds__(512, 1) k_persist(const PhaseDesc *ph, int nph
   }
 }
 
+// Whether an op has row-layout fast paths (load_row / prep_row / store_row).
+template <class Op, class = void> struct RowFast : std::false_type {};
+template <class Op> struct RowFast<Op, std::void_t<decltype(Op::kRowFast)>> : std::bool_constant<Op::kRowFast> {};
+template <class Op> constexpr bool row_fast() { return RowFast<Op>::value; }
+
 // ---------------------------------------------------------------------------
 // Compile-time-schedule line kernel (hot power-of-two lengths): same phases as
 // k_line, with N, T, the lines per CTA and the radix list fixed.  Not used for
@@ -165,13 +170,27 @@ __global__ void __launch_bounds__(LPC *T, MINB) k_line_ct(const KArgs a) {
   c.ooff = c.valid ? line_off(a.out, (uint32_t)c.line) : 0;
   const bool first_g = Op::kFG && (a.flags & GF_FIRST_DIRECT);
   const bool last_g = Op::kTG && (a.flags & GF_LAST_DIRECT);
+  const LineView<C> s = line_view<C>(a, c.l);
+  if constexpr (row_fast<Op>()) {
+    // row layout: prologue and epilogue with the stages' own thread mapping
+    if (!(a.flags & GF_COLMAP)) {
+      if (!first_g) {
+        Op::template load_row<P, N, T>(a, c, line0);
+        cp_async_wait_all();
+        __syncthreads();
+        Op::template prep_row<P, N, T>(a, c, s.b);
+      }
+      run_stages_ct<P, Op, N, T, Op::kFG, Op::kTG, 1>(S{}, s.b, a, c, Op::first_conj(a), first_g, last_g);
+      if (!last_g) Op::template store_row<P, N, T>(a, c, s.b);
+      return;
+    }
+  }
   if (!first_g) {
     Op::template load<P>(a, line0);
     cp_async_wait_all();
     __syncthreads();
     Op::template prep<P>(a, line0);
   }
-  const LineView<C> s = line_view<C>(a, c.l);
   if (a.flags & GF_COLMAP)
     run_stages_ct<P, Op, N, T, Op::kFG, Op::kTG, LPC>(S{}, s.b, a, c, Op::first_conj(a), first_g, last_g);
   else

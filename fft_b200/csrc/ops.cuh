@@ -170,10 +170,12 @@ GF_DEV void untangle_tile(const KArgs &a, long long line0, F emit, void *sb) {
 struct OpR2CPacked {
   static constexpr bool kConv = false, kFG = true, kTG = false;
   static GF_DEV bool first_conj(const KArgs &) { return false; }
+  // Direct first stage: only launched with unit-stride, pair-aligned rows
+  // (GF_PAIR_ALIGNED), so pair j is one vector at element 2j.
   template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int j) {
     using Rl = typename P::real;
     if (!c.valid) return mkc((Rl)0, (Rl)0);
-    return read_pair<P>(a, c.ioff + 2LL * j * a.in.stride, a.in.stride);
+    return ld_stream(reinterpret_cast<const Cx<P> *>((const Rl *)a.in.ptr + c.ioff) + j);
   }
   template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
   template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
@@ -199,6 +201,51 @@ struct OpR2CPacked {
     }
     untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) { out[base + (long long)k * st] = v; }, sb);
   }
+  // Row-layout fast paths for the compiled-schedule kernels (M = lp.n, T
+  // threads per line; thread c.t of line c.l, line data at sb).
+  static constexpr bool kRowFast = true;
+  template <class P, int M, int T> static GF_DEV void load_row(const KArgs &a, const LineCtx &, long long line0) {
+    load<P>(a, line0);
+  }
+  template <class P, int M, int T> static GF_DEV void prep_row(const KArgs &, const LineCtx &, Cx<P> *) {}
+  template <class P, int M, int T> static GF_DEV void store_row(const KArgs &a, const LineCtx &c, Cx<P> *sb) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    using TW = typename P::tw_t;
+    if (!c.valid) return;
+    constexpr int H = M / 2 + 1;
+    constexpr int IT = (H + T - 1) / T;
+    const TW *tw = (const TW *)a.aux0;
+    C *out = (C *)a.out.ptr + c.ooff;
+    const int st = (int)a.out.stride;
+    const Rl half = (Rl)0.5;
+    const bool wgt = (a.ic & GF_EDGE_WEIGHT) != 0;
+    const Rl sc = (Rl)a.scale;
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+      const int k = c.t + it * T;
+      if (IT * T > H && k >= H) break;
+      if (k == 0) {
+        const C z0 = sb[0];
+        const Rl w = wgt ? sc : (Rl)1;
+        out[0] = mkc((z0.x + z0.y) * w, (Rl)0);
+        out[M * st] = mkc((z0.x - z0.y) * w, (Rl)0);
+        continue;
+      }
+      const C zk = sb[spad(k)], zm = sb[spad(M - k)];
+      const C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
+      const C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
+      const C t = twmul(xo, ld_keep(&tw[k]));
+      C lo = cadd(xe, t), hi = mkc(xe.x - t.x, t.y - xe.y);
+      if (wgt) {
+        const Rl w2 = (Rl)2 * sc;
+        lo = mkc(lo.x * w2, lo.y * w2);
+        hi = mkc(hi.x * w2, hi.y * w2);
+      }
+      out[k * st] = lo;
+      if (M - k != k) out[(M - k) * st] = hi;
+    }
+  }
 };
 
 // Even-length real inverse: bins 0..m (fewer if ic < m+1: missing bins read
@@ -214,14 +261,8 @@ struct OpC2RPacked {
     if (!c.valid) return;
     Rl *out = (Rl *)a.out.ptr;
     const Rl sc = (Rl)a.scale;
-    const long long st = a.out.stride;
-    const long long base = c.ooff + 2LL * j * st;
-    if (a.ic & GF_PAIR_ALIGNED) {
-      *reinterpret_cast<Cx<P> *>(&out[base]) = mkc(y.x * sc, -y.y * sc);
-    } else {
-      out[base] = y.x * sc;
-      out[base + st] = -y.y * sc;
-    }
+    // direct last stage: only launched with unit-stride, pair-aligned rows
+    reinterpret_cast<Cx<P> *>(out + c.ooff)[j] = mkc(y.x * sc, -y.y * sc);
   }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     const int m = a.lp.n;
@@ -272,6 +313,59 @@ struct OpC2RPacked {
       out[base + st] = -y.y * sc;
     });
   }
+  // Row-layout fast paths for the compiled-schedule kernels (M = lp.n).
+  static constexpr bool kRowFast = true;
+  template <class P, int M, int T> static GF_DEV void load_row(const KArgs &a, const LineCtx &c, long long) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    constexpr int IT = (M + 1 + T - 1) / T;
+    C *d = line_view<C>(a, c.l).b;
+    if (!c.valid) return;
+    const C *in = (const C *)a.in.ptr + c.ioff;
+    const int st = (int)a.in.stride;
+    const int nb = a.ic & GF_IC_MASK;
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+      const int k = c.t + it * T;
+      if (IT * T > M + 1 && k > M) break;
+      if (k < nb) cp_async_n<sizeof(C)>(&d[spad(k)], &in[k * st]);
+      else d[spad(k)] = mkc((Rl)0, (Rl)0);
+    }
+  }
+  template <class P, int M, int T> static GF_DEV void prep_row(const KArgs &a, const LineCtx &c, Cx<P> *s) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    using TW = typename P::tw_t;
+    constexpr int H = M / 2 + 1;
+    constexpr int IT = (H + T - 1) / T;
+    const TW *tw = (const TW *)a.aux0;
+    const Rl half = (Rl)0.5;
+    const bool wgt = (a.ic & GF_EDGE_WEIGHT) != 0;
+    if (c.valid) {
+#pragma unroll
+      for (int it = 0; it < IT; it++) {
+        const int k = c.t + it * T;
+        if (IT * T > H && k >= H) break;
+        if (k == 0) {
+          const Rl x0 = s[0].x, xm = s[spad(M)].x;
+          s[0] = mkc((x0 + xm) * half, -(x0 - xm) * half);
+          continue;
+        }
+        C xk = s[spad(k)], xmk = s[spad(M - k)];
+        if (wgt) {
+          xk = mkc(xk.x * half, xk.y * half);
+          xmk = mkc(xmk.x * half, xmk.y * half);
+        }
+        const C xe = mkc((xk.x + xmk.x) * half, (xk.y - xmk.y) * half);
+        const C d = mkc((xk.x - xmk.x) * half, (xk.y + xmk.y) * half);
+        const C xo = twmul(d, cconj_tw(ld_keep(&tw[k])));
+        s[spad(k)] = cconj(mkc(xe.x - xo.y, xe.y + xo.x));
+        if (M - k != k) s[spad(M - k)] = cconj(mkc(xe.x + xo.y, -(xe.y - xo.x)));
+      }
+    }
+    __syncthreads();
+  }
+  template <class P, int M, int T> static GF_DEV void store_row(const KArgs &a, const LineCtx &, Cx<P> *) {}
 };
 
 // Odd (or any) length real forward through a full complex line: reals in the

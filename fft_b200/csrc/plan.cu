@@ -546,6 +546,10 @@ static bool side_col(const Side &s) {
 }
 int choose_flags(int op, const KArgs &a) {
   if (op == OP_FILTER_COL) return side_col(a.in) ? GF_COLMAP : 0;
+  // the packed real rows read (R2C) / write (C2R) pairs directly only when
+  // they are unit-stride and pair-aligned
+  if (op == OP_R2C && !(a.ic & GF_PAIR_ALIGNED)) return side_col(a.in) ? GF_COLMAP : 0;
+  if (op == OP_C2R && !(a.ic & GF_PAIR_ALIGNED)) return side_col(a.out) ? GF_COLMAP : 0;
   if (op >= OP_RADER_FS1) return 0;  // gathers and scatters: row layout
   const bool fg = op_fg(op), tg = op_tg(op);
   const bool ic = side_col(a.in), oc = side_col(a.out);
