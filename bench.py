@@ -240,6 +240,155 @@ def time_pipeline(plan, x, spec, back, steps, warmup, world, flush=None):
     return e0.elapsed_time(e1) / 1e3
 
 
+def _events_ms(torch, fn, reps, warm=3):
+    """Average device time of fn() over reps runs (CUDA events, current stream)."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _rel(got, want):
+    got = np.asarray(got, np.complex128).ravel()
+    want = np.asarray(want, np.complex128).ravel()
+    return float(np.linalg.norm(got - want) / np.linalg.norm(want))
+
+
+def extra_workloads(peak):
+    """The other configurations of the transform path, each timed on the
+    device with CUDA events and checked against the oracle on a sample:
+    batched 1-D FFT (256 x 1024 complex128), an uneven batch of 4096 complex64
+    signals (persistent launch and CUDA-graph replay), FFTN of 256^3
+    complex64, the 2^22-sample float32 spectrogram, and the 2-D spectral
+    filter (32 x 512 x 512 float32) forward and backward."""
+    import torch
+    from oracle import oracle as O
+    from fft_b200 import tune
+    from fft_b200.device import DevicePlan, Graph, UnevenBatch, spectrogram
+    from fft_b200.function import SpectralFilter2
+    O.set_workers(0)
+    res = {}
+
+    def line(ms, nbytes, extra):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        d = {"ms": round(ms, 4), "gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 4)}
+        d.update(extra)
+        return d
+
+    # C1: 256 x 1024 complex128, U[-1,1) seed 0, forward then inverse; the
+    # 4 MB batch fits L2, so steps rotate over 64 buffer sets (512 MB)
+    g = np.random.default_rng(0)
+    x1 = g.uniform(-1, 1, (256, 1024)) + 1j * g.uniform(-1, 1, (256, 1024))
+    p1 = DevicePlan("c2c", "f64", [1024], batch=256)
+    K = 64
+    xs = [torch.from_numpy(x1).cuda() for _ in range(K)]
+    ys = [torch.empty_like(xs[0]) for _ in range(K)]
+
+    def c1():
+        for i in range(K):
+            p1.c2c(xs[i], out=ys[i])
+            p1.c2c(ys[i], out=xs[i], inverse=True)
+    ms = _events_ms(torch, c1, 5) / K
+    hot = _events_ms(torch, lambda: (p1.c2c(xs[0], out=ys[0]), p1.c2c(ys[0], out=xs[0], inverse=True)), 50)
+    p1.c2c(torch.from_numpy(x1).cuda(), out=ys[0])
+    rel = _rel(ys[0][:16].cpu().numpy(), O.batch_fft(x1[:16]))
+    gfl = 2 * 256 * 5 * 1024 * 10 / (ms / 1e3) / 1e9
+    res["c1_fft_256x1024_c128"] = line(ms, 16777216, {"l2_hot_ms": round(hot, 4), "gflops_5nlogn": round(gfl, 1),
+                                                      "rel_l2_vs_oracle": rel, "dtype": "f64",
+                                                      "note": "forward+inverse, rotation over 64 buffer sets"})
+    del xs, ys
+
+    # C3: 4096 complex64 signals, lengths uniform over 8 lengths, seed 2
+    g = np.random.default_rng(2)
+    lens = [int(v) for v in g.choice([60, 128, 360, 1000, 1009, 4096, 10007, 65536], 4096)]
+    tot = sum(lens)
+    flat = (g.uniform(-1, 1, tot) + 1j * g.uniform(-1, 1, tot)).astype(np.complex64)
+    tune.autotune_uneven("f32mixed", lens)
+    u = UnevenBatch("f32mixed", lens)
+    xin = torch.from_numpy(flat).cuda()
+    yout = torch.empty_like(xin)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        ms = _events_ms(torch, lambda: u(xin, out=yout, stream=s), 20)
+        with Graph(s) as gr:
+            u(xin, out=yout, stream=s)
+        msg = _events_ms(torch, gr.replay, 20)
+    torch.cuda.synchronize()
+    got = yout.cpu().numpy()
+    offs = np.concatenate([[0], np.cumsum(lens)])
+    pick = [int(i) for i in np.random.default_rng(9).choice(len(lens), 24, replace=False)]
+    rel = max(_rel(got[offs[i]:offs[i + 1]], O.fft(flat[offs[i]:offs[i + 1]].astype(np.complex128))) for i in pick)
+    res["c3_uneven_4096_c64"] = line(ms, tot * 16, {"graph_replay_ms": round(msg, 4), "points": tot,
+                                                    "status": u.status(), "max_rel_l2_24_signals": rel,
+                                                    "dtype": "f32mixed", "note": "forward, one persistent launch"})
+    del u, xin, yout
+
+    # C4: FFTN 256^3 complex64 (unit-variance complex Gaussian, seed 3)
+    g = np.random.default_rng(3)
+    x4 = ((g.standard_normal((256, 256, 256)) + 1j * g.standard_normal((256, 256, 256))) / np.sqrt(2))
+    tune.autotune("c2c", "f32mixed", [256, 256, 256], batch=1)
+    p4 = DevicePlan("c2c", "f32mixed", [256, 256, 256])
+    xt = torch.from_numpy(x4.astype(np.complex64)).cuda().reshape(1, -1)
+    yt = torch.empty_like(xt)
+    ms = _events_ms(torch, lambda: p4.c2c(xt, out=yt), 20)
+    rel = _rel(yt.cpu().numpy(), O.fftn(x4.ravel(), [256, 256, 256]))
+    gfl = 5 * 16777216 * 24 / (ms / 1e3) / 1e9
+    res["c4_fftn_256cube_c64"] = line(ms, 268435456, {"gflops_5nlogn": round(gfl, 1), "rel_l2_vs_oracle": rel,
+                                                      "dtype": "f32mixed", "note": "forward"})
+    del xt, yt, p4
+
+    # C4: spectrogram of a 2^22-sample float32 signal, Hann 2048, overlap 1536
+    sig = g.standard_normal(1 << 22).astype(np.float32)
+    win = O.hann(2048)
+    st = torch.from_numpy(sig).cuda()
+    wt = torch.from_numpy(win.astype(np.float32)).cuda()
+    out = spectrogram(st, 2048, 1536, wt, 1.0, "f32mixed")
+    ms = _events_ms(torch, lambda: spectrogram(st, 2048, 1536, wt, 1.0, "f32mixed"), 20)
+    want = O.spectrogram(sig.astype(np.float64), 2048, 1536, win, 1.0)
+    rel = _rel(out.cpu().numpy(), want)
+    res["c4_spectrogram_2p22_f32"] = line(ms, 50352116, {"frames": int(out.shape[0]), "rel_l2_vs_oracle": rel,
+                                                         "dtype": "f32mixed"})
+
+    # C5: y = IRFFT2(H * RFFT2(x)) over 32 float32 512x512 images and its adjoint
+    x5 = np.random.default_rng(4).random((32, 512, 512), dtype=np.float32)
+    kr = np.fft.fftfreq(512, 1.0 / 512)[:, None]
+    kc = np.arange(257)[None, :]
+    phi = np.random.default_rng(5).uniform(0.0, 2.0 * np.pi, (512, 257))
+    H5 = (np.exp(-(kr ** 2 + kc ** 2) / (2.0 * 40.0 ** 2)) * np.exp(1j * phi)).astype(np.complex64)
+    tune.autotune("r2c", "f32mixed", [512, 512], batch=32)
+    f = SpectralFilter2("f32mixed", 512, 512, batch=32)
+    xt = torch.from_numpy(x5).cuda().reshape(32, -1)
+    Ht = torch.from_numpy(H5).cuda().reshape(-1)
+    y = f.Forward(xt, Ht)
+    msf = _events_ms(torch, lambda: f.plan.filter2(xt, Ht, out=y, saved=f.saved), 20)
+    gy = 2 * y
+    # timed with the saved spectra as their own scratch (overwritten; the same
+    # work as a first backward), then a fresh forward for the checked one
+    msb = _events_ms(torch, lambda: f.plan.vjp_filter2(gy, Ht, saved=f.saved, scratch=f.saved), 20)
+    y = f.Forward(xt, Ht)
+    dx, dH = f.plan.vjp_filter2(2 * y, Ht, saved=f.saved)
+    # the gradient of image 0 and its dH term assembled from the oracle
+    X0 = O.rfft2(x5[0].astype(np.float64), 512, 512).reshape(512, 257)
+    y0 = O.irfft2(H5 * X0, 512, 512)
+    G0 = O.rfft2(2 * y0, 512, 512).reshape(512, 257)
+    dx0 = O.irfft2(np.conj(H5.astype(np.complex128)) * G0, 512, 512)
+    rel_y = _rel(y[0].cpu().numpy(), y0)
+    rel_dx = _rel(dx[0].cpu().numpy(), dx0)
+    res["c5_filter_32x512x512_f32"] = {
+        "forward": line(msf, 33554432 * 2 + 1052672, {"note": "x read, y written, H read"}),
+        "backward": line(msb, 33554432 * 2 + 1052672 * 2, {"note": "g read, dx written, H read, dH written"}),
+        "rel_l2_y_image0_vs_oracle": rel_y, "rel_l2_dx_image0_vs_oracle": rel_dx, "dtype": "f32mixed"}
+    tune.forget_wisdom()
+    return res
+
+
 def run_ours(args):
     import torch
     from fft_b200 import _lib
@@ -337,6 +486,7 @@ def run_ours(args):
 
     if rank != 0:
         return 0
+    extra = extra_workloads(peak) if (world == 1 and not args.no_extra) else None
     cpu = cpu_baseline() if world == 1 else None
     clocks = clk.summary()
     line = {
@@ -363,6 +513,7 @@ def run_ours(args):
                                   "gbs": round(r["bytes"] / (r["ms"] / 1e3) / 1e9, 1),
                                   "share": round(r["ms"] / total_ms, 3)} for r in rep]},
         "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu,
+        "other_workloads": extra,
     }
     if world > 1:
         import torch.distributed as dist
@@ -380,6 +531,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--wisdom", default=None, help="import tuning settings instead of autotuning")
     ap.add_argument("--save-wisdom", default=None, help="write the tuning settings used")
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
