@@ -91,6 +91,16 @@ GF_DEV float ld_stream(const float *p) {
   asm("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
   return v;
 }
+GF_DEV double ld_keep(const double *p) {
+  double v;
+  asm("ld.global.nc.L1::evict_last.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+GF_DEV float ld_keep(const float *p) {
+  float v;
+  asm("ld.global.nc.L1::evict_last.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
 GF_DEV double2 ld_keep(const double2 *p) {
   double2 v;
   asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));

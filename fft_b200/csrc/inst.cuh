@@ -50,7 +50,7 @@ template <class P, int GROUP> KFn pick_maxe(int maxe, int op) {
 // gpu_radices() and pick_threads() derive for the length, the default
 // variant first, then the radix-8 variant (8 elements per thread) and the
 // FP32 radix-32 variant (32 elements per thread) for the lengths of the 2-D
-// workloads.
+// workloads, then fewer lines per CTA for small complex batches.
 #define GF_CT_LIST(X)                                                     \
   X(64, 4, 64, 1, 8, 8) X(64, 4, 128, 0, 8, 8)                           \
   X(128, 8, 32, 1, 16, 8) X(128, 8, 64, 0, 16, 8)                        \
@@ -65,7 +65,10 @@ template <class P, int GROUP> KFn pick_maxe(int maxe, int op) {
   X(512, 64, 4, 1, 8, 8, 8) X(512, 64, 8, 0, 8, 8, 8)                    \
   X(1024, 128, 2, 1, 8, 8, 4, 4) X(1024, 128, 4, 0, 8, 8, 4, 4)          \
   X(2048, 256, 1, 1, 8, 8, 8, 4) X(2048, 256, 2, 0, 8, 8, 8, 4)          \
-  X(512, 16, 16, 1, 32, 16) X(1024, 32, 8, 1, 32, 32)
+  X(512, 16, 16, 1, 32, 16) X(1024, 32, 8, 1, 32, 32)                     \
+  X(128, 8, 2, 0, 16, 8) X(256, 16, 2, 0, 16, 16) X(256, 16, 4, 0, 16, 16) \
+  X(512, 32, 2, 0, 8, 8, 8) X(512, 32, 4, 0, 8, 8, 8)                     \
+  X(1024, 64, 1, 0, 16, 8, 8) X(1024, 64, 2, 0, 16, 8, 8)
 
 template <int... Rs> constexpr bool sched_eq(const int *r, int nst) {
   constexpr int a[] = {Rs...};
@@ -101,6 +104,7 @@ template <class P, int GROUP, int N, int T, int L, bool ROWOPS, int... Rs> KFn c
       case OP_C2C: return pipe ? k_line_pp<P, N, T, L, MINB, OpC2C, S> : k_line_ct<P, N, T, L, MINB, OpC2C, S>;
       case OP_C2C_TW:
         return pipe ? k_line_pp<P, N, T, L, MINB, OpC2CTwiddle, S> : k_line_ct<P, N, T, L, MINB, OpC2CTwiddle, S>;
+      case OP_FILTER_COL: return pipe ? nullptr : k_line_ct<P, N, T, L, MINB, OpFilterCol, S>;
       default: return nullptr;
     }
   } else if constexpr (ROWOPS) {

@@ -171,6 +171,25 @@ __global__ void __launch_bounds__(LPC *T, MINB) k_line_ct(const KArgs a) {
   const bool first_g = Op::kFG && (a.flags & GF_FIRST_DIRECT);
   const bool last_g = Op::kTG && (a.flags & GF_LAST_DIRECT);
   const LineView<C> s = line_view<C>(a, c.l);
+  if constexpr (Op::kConv) {
+    // convolution ops: prologue, forward schedule, the op's middle step, the
+    // schedule again (on conjugated data), epilogue
+    Op::template load<P>(a, line0);
+    cp_async_wait_all();
+    __syncthreads();
+    Op::template prep<P>(a, line0);
+    if (a.flags & GF_COLMAP) {
+      run_stages_ct<P, Op, N, T, false, false, LPC>(S{}, s.b, a, c, Op::first_conj(a), false, false);
+      Op::template mid<P>(a, line0, false);
+      run_stages_ct<P, Op, N, T, false, false, LPC>(S{}, s.b, a, c, false, false, false);
+    } else {
+      run_stages_ct<P, Op, N, T, false, false, 1>(S{}, s.b, a, c, Op::first_conj(a), false, false);
+      Op::template mid<P>(a, line0, false);
+      run_stages_ct<P, Op, N, T, false, false, 1>(S{}, s.b, a, c, false, false, false);
+    }
+    Op::template store<P>(a, line0);
+    return;
+  }
   if constexpr (row_fast<Op>()) {
     // row layout: prologue and epilogue with the stages' own thread mapping
     if (!(a.flags & GF_COLMAP)) {

@@ -666,8 +666,9 @@ struct OpSpectro {
     using Rl = typename P::real;
     if (!c.valid) return mkc((Rl)0, (Rl)0);
     const Rl *win = (const Rl *)a.aux1;
-    const Cx<P> v = read_pair<P>(a, c.ioff + 2LL * j, 1);
-    return mkc(v.x * __ldg(&win[2 * j]), v.y * __ldg(&win[2 * j + 1]));
+    // direct first stage only for pair-aligned frames: pair j is one vector
+    const Cx<P> v = ld_stream(reinterpret_cast<const Cx<P> *>((const Rl *)a.in.ptr + c.ioff) + j);
+    return mkc(v.x * ld_keep(&win[2 * j]), v.y * ld_keep(&win[2 * j + 1]));
   }
   template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
   template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
@@ -699,6 +700,45 @@ struct OpSpectro {
       if (k != 0 && k != m) pw *= (Rl)2;
       out[base + k] = pw;
     }, sb);
+  }
+  // Row-layout fast paths for the compiled-schedule kernels (M = lp.n).
+  static constexpr bool kRowFast = true;
+  template <class P, int M, int T> static GF_DEV void load_row(const KArgs &a, const LineCtx &, long long line0) {
+    load<P>(a, line0);
+  }
+  template <class P, int M, int T> static GF_DEV void prep_row(const KArgs &a, const LineCtx &, Cx<P> *) {
+    prep<P>(a, 0);
+  }
+  template <class P, int M, int T> static GF_DEV void store_row(const KArgs &a, const LineCtx &c, Cx<P> *sb) {
+    using C = Cx<P>;
+    using Rl = typename P::real;
+    using TW = typename P::tw_t;
+    if (!c.valid) return;
+    constexpr int H = M / 2 + 1;
+    constexpr int IT = (H + T - 1) / T;
+    const TW *tw = (const TW *)a.aux0;
+    Rl *out = (Rl *)a.out.ptr + c.ooff;
+    const Rl half = (Rl)0.5;
+    const Rl sc = (Rl)a.scale, sc2 = (Rl)2 * (Rl)a.scale;
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+      const int k = c.t + it * T;
+      if (IT * T > H && k >= H) break;
+      if (k == 0) {
+        const C z0 = sb[0];
+        const Rl d0 = z0.x + z0.y, dm = z0.x - z0.y;
+        out[0] = d0 * d0 * sc;
+        out[M] = dm * dm * sc;
+        continue;
+      }
+      const C zk = sb[spad(k)], zm = sb[spad(M - k)];
+      const C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
+      const C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
+      const C t = twmul(xo, ld_keep(&tw[k]));
+      const C lo = cadd(xe, t), hi = mkc(xe.x - t.x, t.y - xe.y);
+      out[k] = (lo.x * lo.x + lo.y * lo.y) * sc2;
+      if (M - k != k) out[M - k] = (hi.x * hi.x + hi.y * hi.y) * sc2;
+    }
   }
 };
 

@@ -136,6 +136,13 @@ int get_sched_variant(int prec, long long n) {
 }
 // Cache-key part of the settings: the override epoch and the thread's cap.
 int sched_epoch() { return g_sched_epoch.load() * 4 + t_sched_cap; }
+// Uneven-batch execution per precision: persistent kernel (1) or one launch
+// per phase (0); -1 = not set (persistent).
+static std::atomic<int> g_uneven_mode[3] = {{-1}, {-1}, {-1}};
+void set_uneven_mode(int prec, int mode) {
+  if (prec >= 0 && prec < 3) g_uneven_mode[prec].store(mode);
+}
+int get_uneven_mode(int prec) { return (prec >= 0 && prec < 3) ? g_uneven_mode[prec].load() : -1; }
 std::vector<std::array<long long, 3>> list_sched_variants() {
   std::lock_guard<std::mutex> lk(g_sched_mu);
   std::vector<std::array<long long, 3>> v;
@@ -194,7 +201,7 @@ static KFn kernel_for(int prec, int maxe, int op) {
 }
 
 static KFn kernel_ct_for(const DevProg &dp, int op, int lpc, bool pipe) {
-  const bool g0 = op == OP_C2C || op == OP_C2C_TW;
+  const bool g0 = op == OP_C2C || op == OP_C2C_TW || op == OP_FILTER_COL;
   const int n = dp.n, T = dp.lp.T, nst = dp.lp.nst;
   const int *r = dp.lp.radix;
   switch (dp.prec) {
@@ -480,6 +487,7 @@ std::vector<std::array<long long, 4>> list_pipe_overrides() {
   return v;
 }
 void clear_overrides() {
+  for (auto &m : g_uneven_mode) m.store(-1);
   {
     std::lock_guard<std::mutex> lk(g_lpc_mu);
     g_lpc.clear();
@@ -513,6 +521,9 @@ int choose_lpc(const DevProg &dp, const KArgs &a, int op, long long nlines, bool
       const int cap = (int)std::min<size_t>(512 / T, smax / line_bytes);
       lpc = std::max(lpc, std::min(want, cap));
     }
+    // small batches: fewer lines per CTA until the grid covers the SMs
+    // (powers of two, the lines-per-CTA values the compiled kernels have)
+    while (lpc > 1 && (nlines + lpc - 1) / lpc < num_sms() && (lpc & (lpc - 1)) == 0) lpc /= 2;
   }
   lpc = std::min(lpc, std::max(1, 512 / T));
   while (lpc > 1 && (size_t)lpc * line_bytes > smax) lpc--;
@@ -548,7 +559,7 @@ int choose_flags(int op, const KArgs &a) {
   if (op == OP_FILTER_COL) return side_col(a.in) ? GF_COLMAP : 0;
   // the packed real rows read (R2C) / write (C2R) pairs directly only when
   // they are unit-stride and pair-aligned
-  if (op == OP_R2C && !(a.ic & GF_PAIR_ALIGNED)) return side_col(a.in) ? GF_COLMAP : 0;
+  if ((op == OP_R2C || op == OP_SPECTRO) && !(a.ic & GF_PAIR_ALIGNED)) return side_col(a.in) ? GF_COLMAP : 0;
   if (op == OP_C2R && !(a.ic & GF_PAIR_ALIGNED)) return side_col(a.out) ? GF_COLMAP : 0;
   if (op >= OP_RADER_FS1) return 0;  // gathers and scatters: row layout
   const bool fg = op_fg(op), tg = op_tg(op);
@@ -585,9 +596,9 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   static const bool env_pipe = getenv("GOFFT_PIPE") && getenv("GOFFT_PIPE")[0] == '1';
   const bool no_pipe = !(env_pipe || get_pipe_override(dp.prec, dp.n, op));
   long long grid = (nlines + lpc - 1) / lpc;
-  if (!conv && !no_ct) {
+  if (!no_ct) {
     // persistent double-buffered variant when two tile buffers fit
-    if (!no_pipe && 2 * smem <= max_smem_optin() && grid > 2 * num_sms()) {
+    if (!conv && !no_pipe && 2 * smem <= max_smem_optin() && grid > 2 * num_sms()) {
       f = kernel_ct_for(dp, op, lpc, true);
       if (f) {
         if (int rc = ensure_smem(f, 2 * smem)) return rc;

@@ -60,6 +60,8 @@ std::vector<std::array<long long, 3>> list_sched_variants();        // prec, n, 
 std::vector<std::array<long long, 5>> list_lpc_overrides();         // prec, n, op, colmode, lpc
 std::vector<std::array<long long, 4>> list_pipe_overrides();        // prec, n, op, on
 void clear_overrides();
+void set_uneven_mode(int prec, int mode);  // 1 persistent, 0 per phase, -1 unset
+int get_uneven_mode(int prec);
 
 struct DevProg {
   int n = 0, prec = 0, maxe = 16, device = 0;

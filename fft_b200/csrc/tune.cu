@@ -168,6 +168,14 @@ std::string wisdom_json() {
     o << (f ? "" : ",") << "[" << e[0] << "," << e[1] << "," << e[2] << "," << e[3] << "]";
     f = false;
   }
+  o << "],\"uneven\":[";
+  f = true;
+  for (int pr = 0; pr < 3; pr++) {
+    const int m = get_uneven_mode(pr);
+    if (m < 0) continue;
+    o << (f ? "" : ",") << "[" << pr << "," << m << "]";
+    f = false;
+  }
   o << "]}";
   return o.str();
 }
@@ -344,6 +352,14 @@ extern "C" int64_t gofft_autotune_uneven(int precision, const int64_t *lengths, 
       }
     }
   }
+  // persistent launch or one launch per phase
+  if (!rc) {
+    const int cur = get_uneven_mode(precision);
+    set_uneven_mode(precision, cur == 0 ? 1 : 0);
+    double t = 0;
+    if (measure(&t) == 0 && t < best * 0.98) best = t;
+    else set_uneven_mode(precision, cur);
+  }
   cudaStreamDestroy(s);
   if (rc) return -rc;
   return put_string(wisdom_json(), wisdom, cap);
@@ -355,9 +371,12 @@ extern "C" int gofft_wisdom_import(const char *json) {
   if (!json) return set_err(GOFFT_EINVAL, "null wisdom");
   const std::string js(json);
   if (js.find("\"gofft_wisdom\"") == std::string::npos) return set_err(GOFFT_EINVAL, "not gofft wisdom");
-  std::vector<std::vector<long long>> sc, lp, pp;
-  if (!parse_tuples(js, "schedule", 3, sc) || !parse_tuples(js, "lpc", 5, lp) || !parse_tuples(js, "pipe", 4, pp))
+  std::vector<std::vector<long long>> sc, lp, pp, un;
+  if (!parse_tuples(js, "schedule", 3, sc) || !parse_tuples(js, "lpc", 5, lp) || !parse_tuples(js, "pipe", 4, pp) ||
+      !parse_tuples(js, "uneven", 2, un))
     return set_err(GOFFT_EINVAL, "malformed wisdom");
+  for (auto &t : un)
+    if (t[0] < 0 || t[0] > 2 || t[1] < 0 || t[1] > 1) return set_err(GOFFT_EINVAL, "bad uneven entry");
   for (auto &t : sc)
     if (t[0] < 0 || t[0] > 2 || t[1] < 1 || t[2] < 0 || t[2] > 2) return set_err(GOFFT_EINVAL, "bad schedule entry");
   for (auto &t : lp)
@@ -368,6 +387,7 @@ extern "C" int gofft_wisdom_import(const char *json) {
   for (auto &t : sc) set_sched_variant((int)t[0], t[1], (int)t[2]);
   for (auto &t : lp) set_lpc_override((int)t[0], t[1], (int)t[2], (int)t[3], (int)t[4]);
   for (auto &t : pp) set_pipe_override((int)t[0], t[1], (int)t[2], (int)t[3]);
+  for (auto &t : un) set_uneven_mode((int)t[0], (int)t[1]);
   return GOFFT_OK;
 }
 

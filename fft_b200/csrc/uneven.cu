@@ -193,6 +193,7 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
   if (precision < 0 || precision > 2) return set_err(GOFFT_EINVAL, "bad precision");
   std::unique_ptr<gofft_uneven> u(new gofft_uneven());
   u->prec = precision;
+  if (get_uneven_mode(precision) == 0) u->persistent = 0;  // the tuner's choice
   u->count = count;
   cudaGetDevice(&u->device);
   std::vector<long long> ioff(count), ooff(count);

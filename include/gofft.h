@@ -308,11 +308,14 @@ GOFFT_API int gofft_get_schedule(int precision, int64_t n);
 GOFFT_API int64_t gofft_autotune(int kind, int precision, const int64_t *shape, int rank, int64_t batch,
                                  char *wisdom, int64_t cap);
 /* The same for an uneven batch (gofft_uneven_create's lengths): the schedule
- * variant of each length class. */
+ * variant of each length class, then the persistent launch against one
+ * launch per phase (the default for uneven batches of that precision created
+ * afterwards; gofft_uneven_set can still change one batch). */
 GOFFT_API int64_t gofft_autotune_uneven(int precision, const int64_t *lengths, int64_t count, char *wisdom,
                                         int64_t cap);
 /* Current wisdom as JSON: {"gofft_wisdom":1,"schedule":[[prec,n,variant],..],
- * "lpc":[[prec,n,op,colmode,lpc],..],"pipe":[[prec,n,op,on],..]}. */
+ * "lpc":[[prec,n,op,colmode,lpc],..],"pipe":[[prec,n,op,on],..],
+ * "uneven":[[prec,persistent],..]}. */
 GOFFT_API int64_t gofft_wisdom_export(char *buf, int64_t cap);
 /* Applies exported wisdom (entries are added to / replace the current
  * settings); GOFFT_EINVAL on a malformed document, nothing applied then. */

@@ -103,11 +103,11 @@ def test_wisdom_roundtrip():
     from fft_b200._lib import GoFFTError, lib
     tune.forget_wisdom()
     w = {"gofft_wisdom": 1, "schedule": [[0, 512, 1], [2, 1024, 1]], "lpc": [[0, 1024, 0, 1, 8]],
-         "pipe": [[1, 256, 0, 1]]}
+         "pipe": [[1, 256, 0, 1]], "uneven": [[2, 0]]}
     tune.import_wisdom(w)
     got = json.loads(tune.export_wisdom())
     assert sorted(got["schedule"]) == sorted(w["schedule"])
-    assert got["lpc"] == w["lpc"] and got["pipe"] == w["pipe"]
+    assert got["lpc"] == w["lpc"] and got["pipe"] == w["pipe"] and got["uneven"] == w["uneven"]
     assert lib().gofft_get_schedule(0, 512) == 1 and lib().gofft_get_schedule(0, 1024) == 0
     for bad in ['{"schedule": [[0, 512, 1]]}', '{"gofft_wisdom":1,"schedule":[[0,512]]}',
                 '{"gofft_wisdom":1,"schedule":[[0,512,7]]}', '{"gofft_wisdom":1,"lpc":[[0,1,99,0,4]]}']:
@@ -115,4 +115,4 @@ def test_wisdom_roundtrip():
             tune.import_wisdom(bad)
     tune.forget_wisdom()
     got = json.loads(tune.export_wisdom())
-    assert got["schedule"] == [] and got["lpc"] == [] and got["pipe"] == []
+    assert got["schedule"] == [] and got["lpc"] == [] and got["pipe"] == [] and got["uneven"] == []
