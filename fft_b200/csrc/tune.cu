@@ -2,9 +2,10 @@
 //
 // No counterpart in go-fft/fft (its plans are fixed by plan.go's router).
 // For a plan shape the tuner times candidate settings on the device --
-// the radix-schedule variant of every line length the plan uses, then the
-// lines per CTA of its line kernels -- keeps the fastest, and leaves it set
-// for plans created afterwards.  The settings are process-wide per
+// the radix-schedule variant of every line length the plan uses, the lines
+// per CTA of its line kernels, then the double-buffered persistent kernel
+// per pass -- keeps the fastest, and leaves it set for plans created
+// afterwards.  The settings are process-wide per
 // (precision, length[, op, layout]), like FFTW's wisdom, and export to and
 // import from a small JSON document.
 #include <algorithm>
@@ -290,6 +291,16 @@ extern "C" int64_t gofft_autotune(int kind, int precision, const int64_t *shape,
       }
     }
     set_lpc_override(precision, ps.n, ps.op, ps.colmode, keep);
+  }
+  // 3. the persistent double-buffered kernel per pass (prefetches the next
+  //    tile while the current one is transformed)
+  for (size_t pi = 0; pi < passes.size() && !rc; pi++) {
+    const Pass &ps = passes[pi];
+    if (get_pipe_override(precision, ps.n, ps.op)) continue;
+    set_pipe_override(precision, ps.n, ps.op, 1);
+    double t = 0;
+    if (time_plan(kind, precision, sh, batch, s, &t) == 0 && t < best * 0.98) best = t;
+    else set_pipe_override(precision, ps.n, ps.op, 0);
   }
   cudaStreamDestroy(s);
   if (rc) return -rc;

@@ -299,7 +299,8 @@ GOFFT_API int gofft_get_schedule(int precision, int64_t n);
 /* Autotuner (no counterpart in the reference, whose plans are fixed by
  * plan.go's router).  Times candidate settings for batch transforms of
  * `shape` on the current device -- the radix-schedule variant of each line
- * length, then the lines per CTA of each pass -- keeps the fastest, and
+ * length, the lines per CTA of each pass, then the double-buffered
+ * persistent kernel per pass -- keeps the fastest, and
  * leaves them set for plans created afterwards (process-wide per precision
  * and length, like FFTW wisdom).  Allocates its own buffers; takes one forward
  * and inverse transform per candidate.  Writes the resulting wisdom (JSON)
