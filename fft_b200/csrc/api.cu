@@ -710,6 +710,7 @@ static int spectro_dev(int prec, const void *x, int64_t nx, int64_t seg, int64_t
   a.in = mk_side((void *)x, seg - overlap, 0, 1, 1);
   a.out = mk_side(out, m + 1, 0, 1, 1);
   a.aux0 = rx->tw2;
+  a.aux2 = rx->tw2_hi;
   a.aux1 = win;
   a.scale = d / (double)seg;
   a.ic = pairs_aligned(a.in, prec) ? GF_PAIR_ALIGNED : 0;

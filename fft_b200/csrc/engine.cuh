@@ -22,6 +22,7 @@
 // gather the stage cannot express use the cooperative tile loops with
 // asynchronous copies instead.
 #pragma once
+#include <type_traits>
 #include "codelets.cuh"
 
 #define GF_MAXST 24
@@ -43,7 +44,17 @@ struct LineProg {
   int twoff[GF_MAXST];  // offset of the stage's twiddle planes in tw
   FastDiv nsdiv[GF_MAXST];
   const void *tw;       // per-stage twiddles: plane (r-1) holds W_{Ns R}^{k r}, k < Ns
+  const void *tw_hi;    // FP32-mixed programs: the same table as FP32 hi parts only
 };
+
+// FP32-mixed lines up to this length apply the hi parts of their FP64-derived
+// twiddles with plain products (one FP32 rounding per twiddle keeps them well
+// inside the 1e-6 relative-L2 budget); longer lines use the compensated
+// hi+lo products.
+#define GF_F32C_SHORT_MAX 4096
+template <class P, int N> constexpr bool short_tw() {
+  return std::is_same<typename P::tw_t, float4>::value && N <= GF_F32C_SHORT_MAX;
+}
 
 // Addressing of one side of a batched, strided set of lines (in elements).
 // line l, element i:  base(l / lpb) + (l % lpb) * dist_l + i * stride, with
@@ -375,7 +386,7 @@ template <int STEP, class C> GF_DEV C &slot(C *b, int i) { return b[spad(i) * ST
 
 template <class P, class Op, int N, int T, int NS, int R, int E, bool FG, bool TG, int STEP>
 GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &a, const LineCtx &c,
-                     const typename P::tw_t *tw, bool cj) {
+                     const typename P::tw_t *tw, const float2 *twh, bool cj) {
   using C = typename P::cpx;
   constexpr int NB = N / R;
   constexpr int PER = (NB + T - 1) / T;
@@ -411,9 +422,14 @@ GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &
     if (EXACT || j < NB) {
       const int q = j / NS, k = j % NS;
       if constexpr (NS > 1) {
+        if constexpr (short_tw<P, N>()) {
 #pragma unroll
-        for (int r = 1; r < R; r++)
-          v[b * R + r] = twmul(v[b * R + r], ld_keep(&tw[(r - 1) * NS + k]));
+          for (int r = 1; r < R; r++) v[b * R + r] = cmul(v[b * R + r], ld_keep(&twh[(r - 1) * NS + k]));
+        } else {
+#pragma unroll
+          for (int r = 1; r < R; r++)
+            v[b * R + r] = twmul(v[b * R + r], ld_keep(&tw[(r - 1) * NS + k]));
+        }
       }
       Dft<R, C>::run(&v[b * R]);
       const int base = q * NS * R + k;
@@ -441,22 +457,23 @@ GF_DEV void stages_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs 
   constexpr bool FIRST = NS == 1;
   constexpr bool LAST = sizeof...(Rs) == 0;
   const TW *tw = (const TW *)a.lp.tw + TO;
+  const float2 *twh = short_tw<P, N>() ? (const float2 *)a.lp.tw_hi + TO : nullptr;
   const bool cj = FIRST && cj_first;
   constexpr bool F_OK = FIRST && CAN_FG;
   constexpr bool T_OK = LAST && CAN_TG;
   if constexpr (F_OK && T_OK) {
-    if (fg && tg) stage_ct<P, Op, N, T, NS, R, E, true, true, STEP>(v, sb, a, c, tw, cj);
-    else if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP>(v, sb, a, c, tw, cj);
-    else if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP>(v, sb, a, c, tw, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, cj);
+    if (fg && tg) stage_ct<P, Op, N, T, NS, R, E, true, true, STEP>(v, sb, a, c, tw, twh, cj);
+    else if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP>(v, sb, a, c, tw, twh, cj);
+    else if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP>(v, sb, a, c, tw, twh, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, twh, cj);
   } else if constexpr (F_OK) {
-    if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP>(v, sb, a, c, tw, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, cj);
+    if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP>(v, sb, a, c, tw, twh, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, twh, cj);
   } else if constexpr (T_OK) {
-    if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP>(v, sb, a, c, tw, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, cj);
+    if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP>(v, sb, a, c, tw, twh, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, twh, cj);
   } else {
-    stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, cj);
+    stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, twh, cj);
   }
   if constexpr (!LAST)
     stages_ct<P, Op, N, T, NS * R, TO + NS * (R - 1), E, CAN_FG, CAN_TG, STEP, Rs...>(v, sb, a, c, cj_first, fg,

@@ -136,7 +136,8 @@ struct OpC2CTwiddle {
 // Even-length real forward: the 2m reals of a line are read as m complex
 // values z[j] = x[2j] + i x[2j+1]; after the m-point FFT the untangle
 //   X[k] = (Z[k] + conj Z[m-k])/2 + W_2m^k (Z[k] - conj Z[m-k])/(2i)
-// writes bins 0..m (aux0 = W_2m^k table, k = 0..m).  Sides count reals on
+// writes bins 0..m (aux0 = W_2m^k table, k = 0..m; FP32-mixed: aux1 = the
+// same roots as FP32 hi parts, for short lines).  Sides count reals on
 // input and complex bins on output.
 // ---------------------------------------------------------------------------
 template <class P, class F>
@@ -235,7 +236,9 @@ struct OpR2CPacked {
       const C zk = sb[spad(k)], zm = sb[spad(M - k)];
       const C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
       const C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
-      const C t = twmul(xo, ld_keep(&tw[k]));
+      C t;
+      if constexpr (short_tw<P, M>()) t = cmul(xo, ld_keep(&((const float2 *)a.aux1)[k]));
+      else t = twmul(xo, ld_keep(&tw[k]));
       C lo = cadd(xe, t), hi = mkc(xe.x - t.x, t.y - xe.y);
       if (wgt) {
         const Rl w2 = (Rl)2 * sc;
@@ -251,7 +254,8 @@ struct OpR2CPacked {
 // Even-length real inverse: bins 0..m (fewer if ic < m+1: missing bins read
 // as zero; imaginary parts of bins 0 and m ignored) are folded back into the
 // m-point packed spectrum Z, which is inverse transformed (conjugate trick)
-// and unpacked into 2m reals scaled by `scale`.  aux0 = W_2m^k table.
+// and unpacked into 2m reals scaled by `scale`.  aux0 = W_2m^k table
+// (FP32-mixed: aux1 = its FP32 hi parts, for short lines).
 struct OpC2RPacked {
   static constexpr bool kConv = false, kFG = false, kTG = true;
   static GF_DEV bool first_conj(const KArgs &) { return false; }
@@ -358,7 +362,9 @@ struct OpC2RPacked {
         }
         const C xe = mkc((xk.x + xmk.x) * half, (xk.y - xmk.y) * half);
         const C d = mkc((xk.x - xmk.x) * half, (xk.y + xmk.y) * half);
-        const C xo = twmul(d, cconj_tw(ld_keep(&tw[k])));
+        C xo;
+        if constexpr (short_tw<P, M>()) xo = cmul(d, cconj_tw(ld_keep(&((const float2 *)a.aux1)[k])));
+        else xo = twmul(d, cconj_tw(ld_keep(&tw[k])));
         s[spad(k)] = cconj(mkc(xe.x - xo.y, xe.y + xo.x));
         if (M - k != k) s[spad(M - k)] = cconj(mkc(xe.x + xo.y, -(xe.y - xo.x)));
       }
@@ -657,7 +663,8 @@ struct OpBluestein {
 // real line (seg = 2m) and reduced to the one-sided density
 //   p[k] = |X[k]|^2 * scale, doubled except for k = 0 and k = m.
 // in: real signal (Side: dist_b = step per frame, stride 1); aux1 = window
-// (real, seg); aux0 = W_2m^k table; out: real bins (m+1 per frame).
+// (real, seg); aux0 = W_2m^k table (FP32-mixed: aux2 = its FP32 hi parts,
+// for short lines); out: real bins (m+1 per frame).
 // ---------------------------------------------------------------------------
 struct OpSpectro {
   static constexpr bool kConv = false, kFG = true, kTG = false;
@@ -734,7 +741,9 @@ struct OpSpectro {
       const C zk = sb[spad(k)], zm = sb[spad(M - k)];
       const C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
       const C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
-      const C t = twmul(xo, ld_keep(&tw[k]));
+      C t;
+      if constexpr (short_tw<P, M>()) t = cmul(xo, ld_keep(&((const float2 *)a.aux2)[k]));
+      else t = twmul(xo, ld_keep(&tw[k]));
       const C lo = cadd(xe, t), hi = mkc(xe.x - t.x, t.y - xe.y);
       out[k] = (lo.x * lo.x + lo.y * lo.y) * sc2;
       if (M - k != k) out[M - k] = (hi.x * hi.x + hi.y * hi.y) * sc2;

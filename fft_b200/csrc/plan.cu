@@ -244,6 +244,7 @@ static int ensure_smem(KFn f, size_t smem) {
 // ---------------------------------------------------------------------------
 DevProg::~DevProg() {
   if (tw) cudaFree(tw);
+  if (tw_hi) cudaFree(tw_hi);
 }
 
 static int pick_threads(long long n, int maxe, const std::vector<int> &rad) {
@@ -348,6 +349,12 @@ static int build_prog(long long n, int prec, std::shared_ptr<DevProg> &out) {
     default: e = prec_f32c::stage_tw(dp->tw, tab, off, 0); break;
   }
   GF_CK(e);
+  if (prec == F32C) {
+    // the hi parts as a compact FP32 table, for the short-line kernels
+    GF_CK(cudaMalloc(&dp->tw_hi, total * twsize(F32)));
+    lp.tw_hi = dp->tw_hi;
+    GF_CK(prec_f32::stage_tw(dp->tw_hi, tab, off, 0));
+  }
   GF_CK(cudaStreamSynchronize(0));
   out = dp;
   return 0;
@@ -1058,6 +1065,7 @@ std::shared_ptr<const Exec1D> get_exec(long long n, int prec) {
 // ---------------------------------------------------------------------------
 ExecReal::~ExecReal() {
   if (tw2) cudaFree(tw2);
+  if (tw2_hi) cudaFree(tw2_hi);
 }
 
 size_t ExecReal::ws_bytes(long long nl) const {
@@ -1080,6 +1088,7 @@ int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaS
       a.in = in;
       a.out = out;
       a.aux0 = tw2;
+      a.aux1 = tw2_hi;
       a.scale = wsc != 0.0 ? wsc : 1.0;
       a.ic = (pairs_aligned(in, prec) ? GF_PAIR_ALIGNED : 0) | (wsc != 0.0 ? GF_EDGE_WEIGHT : 0);
       return launch_line(OP_R2C, *cx->prog, a, nl, st);
@@ -1126,6 +1135,7 @@ int ExecReal::c2r(const Side &in, int nb, const Side &out, long long nl, double 
       a.in = in;
       a.out = out;
       a.aux0 = tw2;
+      a.aux1 = tw2_hi;
       a.ic = nb | (pairs_aligned(out, prec) ? GF_PAIR_ALIGNED : 0) | (halve ? GF_EDGE_WEIGHT : 0);
       a.scale = scale / (double)m;
       return launch_line(OP_C2R, *cx->prog, a, nl, st);
@@ -1179,6 +1189,10 @@ static int build_real(long long n, int prec, std::shared_ptr<ExecReal> &out) {
     r->mode = r->cx->kind == K_SINGLE ? R_PACKED_FUSED : R_PACKED_MULTI;
     GF_CK(cudaMalloc(&r->tw2, (m + 1) * twsize(prec)));
     GF_CK(GF_PREC_CALL(prec, roots, r->tw2, n, m + 1, 0));
+    if (prec == F32C) {
+      GF_CK(cudaMalloc(&r->tw2_hi, (m + 1) * twsize(F32)));
+      GF_CK(GF_PREC_CALL(F32, roots, r->tw2_hi, n, m + 1, 0));
+    }
     GF_CK(cudaStreamSynchronize(0));
   } else {
     r->cx = get_exec(n, prec);

@@ -67,6 +67,7 @@ struct DevProg {
   int n = 0, prec = 0, maxe = 16, device = 0;
   LineProg lp{};
   void *tw = nullptr;
+  void *tw_hi = nullptr;  // FP32-mixed: hi parts as FP32 pairs
   ~DevProg();
 };
 
@@ -114,6 +115,7 @@ struct ExecReal {
   int prec = 0, mode = R_FULL_FUSED, device = 0;
   std::shared_ptr<const Exec1D> cx;  // half (even) or full (odd) complex exec
   void *tw2 = nullptr;               // W_n^k, k = 0..n/2 (packed modes)
+  void *tw2_hi = nullptr;            // FP32-mixed: hi parts as FP32 pairs
   ~ExecReal();
   size_t ws_bytes(long long nlines) const;
   // in: reals, out: bins.  wsc != 0 applies the real-spectrum edge-bin

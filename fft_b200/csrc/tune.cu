@@ -118,7 +118,7 @@ int time_plan(int kind, int prec, const std::vector<long long> &shape, long long
       if (int e = gofft_exec_r2c(p, a.p, b.p, st)) return e;
       return gofft_exec_c2r(p, b.p, 0, a.p, st);
     };
-    rc = time_ms(run, s, 2, 5, ms);
+    rc = time_ms(run, s, 3, 9, ms);
   }
   cudaStreamSynchronize(s);
   gofft_plan_destroy(p);
@@ -338,7 +338,7 @@ extern "C" int64_t gofft_autotune_uneven(int precision, const int64_t *lengths, 
     gofft_uneven *u = nullptr;
     if (int e = gofft_uneven_create(precision, lengths, count, nullptr, nullptr, &u)) return e;
     auto run = [&](cudaStream_t st) -> int { return gofft_uneven_exec(u, a.p, b.p, 0, st); };
-    int e = time_ms(run, s, 2, 5, ms);
+    int e = time_ms(run, s, 3, 9, ms);
     cudaStreamSynchronize(s);
     if (!e && gofft_uneven_status(u) != GOFFT_OK) e = set_err(GOFFT_ETIMEOUT, "tuner run timed out");
     gofft_uneven_destroy(u);
