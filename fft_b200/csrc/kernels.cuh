@@ -172,22 +172,25 @@ __global__ void __launch_bounds__(LPC *T, MINB) k_line_ct(const KArgs a) {
   const bool last_g = Op::kTG && (a.flags & GF_LAST_DIRECT);
   const LineView<C> s = line_view<C>(a, c.l);
   if constexpr (Op::kConv) {
-    // convolution ops: prologue, forward schedule, the op's middle step, the
-    // schedule again (on conjugated data), epilogue
-    Op::template load<P>(a, line0);
-    cp_async_wait_all();
-    __syncthreads();
-    Op::template prep<P>(a, line0);
-    if (a.flags & GF_COLMAP) {
-      run_stages_ct<P, Op, N, T, false, false, LPC>(S{}, s.b, a, c, Op::first_conj(a), false, false);
-      Op::template mid<P>(a, line0, false);
-      run_stages_ct<P, Op, N, T, false, false, LPC>(S{}, s.b, a, c, false, false, false);
-    } else {
-      run_stages_ct<P, Op, N, T, false, false, 1>(S{}, s.b, a, c, Op::first_conj(a), false, false);
-      Op::template mid<P>(a, line0, false);
-      run_stages_ct<P, Op, N, T, false, false, 1>(S{}, s.b, a, c, false, false, false);
+    // convolution ops: forward schedule (first stage from global memory when
+    // the layout allows), the op's middle step, the schedule again on
+    // conjugated data (last stage to global memory when allowed)
+    if (!first_g) {
+      Op::template load<P>(a, line0);
+      cp_async_wait_all();
+      __syncthreads();
+      Op::template prep<P>(a, line0);
     }
-    Op::template store<P>(a, line0);
+    if (a.flags & GF_COLMAP) {
+      run_stages_ct<P, Op, N, T, Op::kFG, false, LPC>(S{}, s.b, a, c, Op::first_conj(a), first_g, false);
+      Op::template mid<P>(a, line0, false);
+      run_stages_ct<P, Op, N, T, false, Op::kTG, LPC>(S{}, s.b, a, c, false, false, last_g);
+    } else {
+      run_stages_ct<P, Op, N, T, Op::kFG, false, 1>(S{}, s.b, a, c, Op::first_conj(a), first_g, false);
+      Op::template mid<P>(a, line0, false);
+      run_stages_ct<P, Op, N, T, false, Op::kTG, 1>(S{}, s.b, a, c, false, false, last_g);
+    }
+    if (!last_g) Op::template store<P>(a, line0);
     return;
   }
   if constexpr (row_fast<Op>()) {

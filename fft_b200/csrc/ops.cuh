@@ -70,16 +70,23 @@ template <class P> GF_DEV void load_bins(const KArgs &a, long long line0, int cn
 struct OpC2C {
   static constexpr bool kConv = false, kFG = true, kTG = true;
   static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
+  // Direct stages: element offsets within a line fit 32 bits (launches whose
+  // line extent n * stride does not are given the tile prologue/epilogue).
   template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int i) {
     using Rl = typename P::real;
     if (!c.valid) return mkc((Rl)0, (Rl)0);
-    return ld_stream(&((const Cx<P> *)a.in.ptr)[c.ioff + (long long)i * a.in.stride]);
+    return ld_stream(&((const Cx<P> *)a.in.ptr + c.ioff)[i * (int)a.in.stride]);
   }
   template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
     using Rl = typename P::real;
     if (!c.valid) return;
+    Cx<P> *o = &((Cx<P> *)a.out.ptr + c.ooff)[i * (int)a.out.stride];
+    if (a.scale == 1.0) {  // forward passes: no multiply
+      *o = a.cj_out ? mkc(y.x, -y.y) : y;
+      return;
+    }
     const Rl sc = (Rl)a.scale;
-    ((Cx<P> *)a.out.ptr)[c.ooff + (long long)i * a.out.stride] = mkc(y.x * sc, y.y * (a.cj_out ? -sc : sc));
+    *o = mkc(y.x * sc, y.y * (a.cj_out ? -sc : sc));
   }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
@@ -896,10 +903,15 @@ struct OpRaderFS4 {  // aux0 iperm, aux1 x0s, aux2 dc; ia = q, ib = off
 #define GF_FILT_DH 4
 
 struct OpFilterCol {
-  static constexpr bool kConv = true, kFG = false, kTG = false;
+  static constexpr bool kConv = true, kFG = true, kTG = true;
   static GF_DEV bool first_conj(const KArgs &) { return false; }
-  template <class P> static GF_DEV Cx<P> gload(const KArgs &, const LineCtx &, int) { return Cx<P>(); }
-  template <class P> static GF_DEV void gstore(const KArgs &, const LineCtx &, int, Cx<P>) {}
+  // direct first stage of the forward FFT and last stage of the inverse
+  template <class P> static GF_DEV Cx<P> gload(const KArgs &a, const LineCtx &c, int i) {
+    return OpC2C::gload<P>(a, c, i);
+  }
+  template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
+    OpC2C::gstore<P>(a, c, i, y);
+  }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     OpC2C::load<P>(a, line0, sb);
   }

@@ -563,7 +563,7 @@ static bool side_col(const Side &s) {
   return std::llabs(D) < std::llabs(s.stride);
 }
 int choose_flags(int op, const KArgs &a) {
-  if (op == OP_FILTER_COL) return side_col(a.in) ? GF_COLMAP : 0;
+  if (op == OP_FILTER_COL) return (side_col(a.in) ? GF_COLMAP : 0) | GF_FIRST_DIRECT | GF_LAST_DIRECT;
   // the packed real rows read (R2C) / write (C2R) pairs directly only when
   // they are unit-stride and pair-aligned
   if ((op == OP_R2C || op == OP_SPECTRO) && !(a.ic & GF_PAIR_ALIGNED)) return side_col(a.in) ? GF_COLMAP : 0;
@@ -591,6 +591,9 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   a.ndiv = FastDiv((uint32_t)dp.n);
   a.lpcdiv = FastDiv((uint32_t)lpc);
   a.flags = choose_flags(op, a);
+  // direct stages index a line with 32-bit element offsets
+  if (std::max(std::llabs(a.in.stride), std::llabs(a.out.stride)) * (long long)dp.n >= (1ll << 31))
+    a.flags &= GF_COLMAP;
   if (const char *e = getenv("GOFFT_NO_DIRECT")) {
     if (*e == '1') a.flags &= GF_COLMAP;
   }
