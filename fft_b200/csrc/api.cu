@@ -27,6 +27,8 @@ struct gofft_plan {
   long long chunk = 1;                            // images per L2 block (rank-2 R2C)
   int nlanes = 1;                                 // streams the blocks alternate on
   size_t lane_bytes = 0;                          // workspace per lane
+  size_t lane_buf = 0;                            // block buffer at the start of a lane region
+  long long nplane_blocks = 0;                    // complex N-D: planes per L2 block (0: unblocked)
   cudaStream_t lane = nullptr;                    // the second lane's stream
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   size_t ws_bytes = 0;
@@ -75,6 +77,16 @@ static int plan_ws(gofft_plan *p) {
       const long long lines = (p->rank == 1 ? p->batch : p->batch * (p->total / p->shape[a]));
       need = std::max(need, p->ax[a]->ws_bytes(lines));
     }
+    if (p->nplane_blocks > 0) {
+      // two lane regions for the blocked last-two-axes passes
+      const int r = p->rank;
+      const long long kb = p->nplane_blocks;
+      const size_t sub = std::max(p->ax[r - 1]->ws_bytes(kb * p->shape[r - 2]),
+                                  p->ax[r - 2]->ws_bytes(kb * p->shape[r - 1]));
+      p->lane_buf = 0;
+      p->lane_bytes = (sub + 255) & ~(size_t)255;
+      need = std::max(need, 2 * p->lane_bytes);
+    }
   } else if (p->rank == 1) {
     need = p->rx->ws_bytes(p->batch);
   } else {
@@ -82,6 +94,7 @@ static int plan_ws(gofft_plan *p) {
     const long long rows = p->shape[0], rc = p->shape[1] / 2 + 1;
     const size_t cols_buf = ((size_t)rows * rc * p->chunk * csize(p->prec) + 255) & ~(size_t)255;
     const size_t sub = std::max(p->rx->ws_bytes(rows * p->chunk), p->ax[0]->ws_bytes(rc * p->chunk));
+    p->lane_buf = cols_buf;
     p->lane_bytes = (cols_buf + sub + 255) & ~(size_t)255;
     need = p->lane_bytes * p->nlanes;
   }
@@ -129,6 +142,21 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       auto ex = get_exec(p->shape[a], precision);
       if (!ex) return GOFFT_ECUDA;
       p->ax.push_back(ex);
+    }
+    if (rank >= 2 && p->shape[rank - 1] > 1 && p->shape[rank - 2] > 1) {
+      // planes (the last two axes) per L2 block: both axes run while a
+      // block's planes sit in L2, on two lanes; leading axes run afterwards
+      const long long plane = p->shape[rank - 1] * p->shape[rank - 2];
+      const bool merged = p->idist == p->total && p->odist == p->total;
+      const long long units = (merged ? batch : 1) * (p->total / plane);
+      const long long budget = env_ll("GOFFT_L2_BLOCK_BYTES", 48ll << 20);
+      const long long cmax =
+          std::max<long long>(1, std::min<long long>(units, budget / (plane * (long long)csize(precision))));
+      const long long nblocks = (units + cmax - 1) / cmax;
+      if (nblocks > 1 && env_ll("GOFFT_LANES", 2) >= 2) {
+        p->nplane_blocks = (units + nblocks - 1) / nblocks;
+        p->nlanes = 2;
+      }
     }
   } else {
     p->rx = get_real(last, precision);
@@ -223,6 +251,39 @@ extern "C" int64_t gofft_plan_table(const gofft_plan *p, int which, int64_t *out
 // ---------------------------------------------------------------------------
 // Execution on device pointers
 // ---------------------------------------------------------------------------
+// The L2 blocks of a plan (images of a rank-2 real plan, planes of a complex
+// N-D plan) alternate between the caller's stream and the plan's lane stream
+// (forked from and joined back into the caller's stream), each lane with its
+// own workspace region: the block buffer (real plans), then the passes'
+// workspace.
+struct Lanes {
+  gofft_plan *p;
+  cudaStream_t st;
+  bool two = false;
+  Lanes(gofft_plan *p_, cudaStream_t st_) : p(p_), st(st_) {}
+  int fork(long long nblocks) {
+    two = p->nlanes > 1 && nblocks > 1;
+    if (!two) return 0;
+    GF_CK(cudaEventRecord(p->ev_fork, st));
+    GF_CK(cudaStreamWaitEvent(p->lane, p->ev_fork, 0));
+    return 0;
+  }
+  cudaStream_t stream(long long blk) const { return (two && (blk & 1)) ? p->lane : st; }
+  char *buf(long long blk) const { return (char *)p->ws + ((two && (blk & 1)) ? p->lane_bytes : 0); }
+  char *sub(long long blk) const { return buf(blk) + p->lane_buf; }
+  // Joins the lane back into the caller's stream; keeps the first error.
+  int join(int rc) {
+    if (!two) return rc;
+    two = false;
+    cudaError_t e1 = cudaEventRecord(p->ev_join, p->lane);
+    cudaError_t e2 = cudaStreamWaitEvent(st, p->ev_join, 0);
+    if (rc) return rc;
+    if (e1 != cudaSuccess || e2 != cudaSuccess)
+      return set_err(GOFFT_ECUDA, std::string("lane join: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    return 0;
+  }
+};
+
 // cj: transform direction (1 = inverse, as conj(FFT(conj .))); scaled: apply
 // the inverse's 1/n per axis.  The plain transforms have cj == scaled; the
 // adjoints flip the direction and keep the scaling.
@@ -236,12 +297,37 @@ static int exec_c2c_dir(gofft_plan *p, const void *in, void *out, int cj, int sc
   const bool merged = p->idist == p->total && p->odist == p->total;
   const long long nb = merged ? 1 : p->batch;
   const long long per = merged ? p->batch : 1;
+  const int r = p->rank;
   for (long long b = 0; b < nb; b++) {
     const char *src = (const char *)in + (size_t)b * p->idist * c;
     char *dst = (char *)out + (size_t)b * p->odist * c;
     bool first = true;
+    int lead = r;  // axes 0..lead-1 still to run over the whole array
+    if (p->nplane_blocks > 0) {
+      // the last two axes per L2 block of planes, blocks alternating lanes
+      const long long Lr = p->shape[r - 1], Lc = p->shape[r - 2], plane = Lr * Lc;
+      const long long units = per * (p->total / plane), kb0 = p->nplane_blocks;
+      Lanes ln(p, st);
+      if (int e = ln.fork((units + kb0 - 1) / kb0)) return e;
+      long long blk = 0;
+      for (long long k0 = 0; k0 < units; k0 += kb0, blk++) {
+        const long long kb = std::min(kb0, units - k0);
+        const size_t off = (size_t)k0 * plane * c;
+        const cudaStream_t s = ln.stream(blk);
+        char *wsx = ln.sub(blk);
+        const Side rin = mk_side((void *)(src + off), Lr, 1, 1, 1), rout = mk_side(dst + off, Lr, 1, 1, 1);
+        if (int e = p->ax[r - 1]->exec(rin, rout, kb * Lc, cj, cj, scaled ? 1.0 / (double)Lr : 1.0, wsx, s))
+          return ln.join(e);
+        const Side cs = mk_side(dst + off, plane, 1, Lr, Lr);
+        if (int e = p->ax[r - 2]->exec(cs, cs, kb * Lr, cj, cj, scaled ? 1.0 / (double)Lc : 1.0, wsx, s))
+          return ln.join(e);
+      }
+      if (int e = ln.join(GOFFT_OK)) return e;
+      first = false;
+      lead = r - 2;
+    }
     long long inner = p->total;
-    for (int a = 0; a < p->rank; a++) {
+    for (int a = 0; a < lead; a++) {
       const long long L = p->shape[a];
       inner /= L;
       if (L == 1) continue;
@@ -261,40 +347,6 @@ static int exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, cudaS
   return exec_c2c_dir(p, in, out, inverse ? 1 : 0, inverse ? 1 : 0, st);
 }
 
-// The L2 blocks of a rank-2 real plan alternate between the caller's stream
-// and the plan's lane stream (forked from and joined back into the caller's
-// stream), each lane with its own workspace region: block spectrum buffer
-// first, then the passes' workspace.
-struct Lanes {
-  gofft_plan *p;
-  cudaStream_t st;
-  bool two = false;
-  Lanes(gofft_plan *p_, cudaStream_t st_) : p(p_), st(st_) {}
-  int fork() {
-    two = p->nlanes > 1 && p->chunk < p->batch;
-    if (!two) return 0;
-    GF_CK(cudaEventRecord(p->ev_fork, st));
-    GF_CK(cudaStreamWaitEvent(p->lane, p->ev_fork, 0));
-    return 0;
-  }
-  cudaStream_t stream(long long blk) const { return (two && (blk & 1)) ? p->lane : st; }
-  char *buf(long long blk) const { return (char *)p->ws + ((two && (blk & 1)) ? p->lane_bytes : 0); }
-  char *sub(long long blk) const {
-    const long long rows = p->shape[0], rc = p->shape[1] / 2 + 1;
-    return buf(blk) + (((size_t)rows * rc * p->chunk * csize(p->prec) + 255) & ~(size_t)255);
-  }
-  // Joins the lane back into the caller's stream; keeps the first error.
-  int join(int rc) {
-    if (!two) return rc;
-    two = false;
-    cudaError_t e1 = cudaEventRecord(p->ev_join, p->lane);
-    cudaError_t e2 = cudaStreamWaitEvent(st, p->ev_join, 0);
-    if (rc) return rc;
-    if (e1 != cudaSuccess || e2 != cudaSuccess)
-      return set_err(GOFFT_ECUDA, std::string("lane join: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
-    return 0;
-  }
-};
 
 // wsc != 0: the adjoint of the inverse (edge-bin weighting with scale wsc on
 // the row pass, the only real one).
@@ -306,7 +358,7 @@ static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st, d
   const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
   const size_t r = rsize(p->prec), c = csize(p->prec);
   Lanes ln(p, st);
-  if (int e = ln.fork()) return e;
+  if (int e = ln.fork((p->batch + p->chunk - 1) / p->chunk)) return e;
   long long blk = 0;
   for (long long b0 = 0; b0 < p->batch; b0 += p->chunk, blk++) {
     const long long nb = std::min(p->chunk, p->batch - b0);
@@ -340,7 +392,7 @@ static int exec_c2r(gofft_plan *p, const void *in, long long nbins, void *out, c
   const long long rows = p->shape[0], cols = last;
   const size_t r = rsize(p->prec), c = csize(p->prec);
   Lanes ln(p, st);
-  if (int e = ln.fork()) return e;
+  if (int e = ln.fork((p->batch + p->chunk - 1) / p->chunk)) return e;
   long long blk = 0;
   for (long long b0 = 0; b0 < p->batch; b0 += p->chunk, blk++) {
     const long long nb = std::min(p->chunk, p->batch - b0);
@@ -904,7 +956,7 @@ static int filter2_run(gofft_plan *p, const void *x, const void *H, void *y, voi
   const Exec1D &cx = *p->ax[0];
   const double dsc = 1.0 / ((double)rows * (double)cols);
   Lanes ln(p, st);
-  if (int e = ln.fork()) return e;
+  if (int e = ln.fork((p->batch + p->chunk - 1) / p->chunk)) return e;
   long long blk = -1;
   for (long long b0 = 0; b0 < p->batch; b0 += p->chunk) {
     blk++;

@@ -165,3 +165,29 @@ def test_device_spectrogram_fp32(prec):
     want = O.spectrogram(x.astype(np.float64), 2048, 1536, w.astype(np.float64), 1.0)
     assert got.shape == want.shape
     assert rel_l2(got.cpu().numpy(), want) <= F32_TOL
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32mixed"])
+@pytest.mark.parametrize("shape,batch,gap", [([40, 64, 96], 1, 0), ([64, 96], 40, 0), ([20, 32, 48], 2, 5),
+                                            ([6, 5, 64, 1009], 1, 0), ([10, 360, 48], 3, 0)])
+def test_fftn_plane_blocks(prec, shape, batch, gap, monkeypatch):
+    """Complex N-D transforms whose last two axes run per L2 block of planes
+    on two lanes (a small block budget forces several blocks), against the
+    oracle: merged and gapped batches, prime and smooth axes."""
+    from fft_b200.device import DevicePlan
+    monkeypatch.setenv("GOFFT_L2_BLOCK_BYTES", str(1 << 20))
+    n = int(np.prod(shape))
+    dist = n + gap
+    g = rng(n + batch)
+    flat = g.standard_normal(batch * dist) + 1j * g.standard_normal(batch * dist)
+    cdt = torch.complex128 if prec == "f64" else torch.complex64
+    tol = F64_TOL if prec == "f64" else F32_TOL
+    p = DevicePlan("c2c", prec, shape, batch=batch, idist=dist, odist=dist)
+    x = torch.from_numpy(flat).to(cdt).cuda()
+    for inverse in (False, True):
+        y = torch.zeros_like(x)
+        p.c2c(x, out=y, inverse=inverse)
+        got = y.cpu().numpy()
+        for b in range(batch):
+            want = O.fftn(flat[b * dist:b * dist + n], shape, inverse=inverse)
+            assert rel_l2(got[b * dist:b * dist + n], want) <= tol, (shape, b, inverse)
