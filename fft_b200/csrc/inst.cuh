@@ -67,8 +67,9 @@ template <class P, int GROUP> KFn pick_maxe(int maxe, int op) {
   X(2048, 256, 1, 1, 8, 8, 8, 4) X(2048, 256, 2, 0, 8, 8, 8, 4)          \
   X(512, 16, 16, 1, 32, 16) X(1024, 32, 8, 1, 32, 32)                     \
   X(128, 8, 2, 0, 16, 8) X(256, 16, 2, 0, 16, 16) X(256, 16, 4, 0, 16, 16) \
-  X(512, 32, 2, 0, 8, 8, 8) X(512, 32, 4, 0, 8, 8, 8)                     \
-  X(1024, 64, 1, 0, 16, 8, 8) X(1024, 64, 2, 0, 16, 8, 8)
+  X(512, 32, 2, 0, 8, 8, 8)                                               \
+  X(1024, 64, 1, 0, 16, 8, 8) X(1024, 64, 2, 0, 16, 8, 8)                 \
+  X(512, 64, 2, 1, 8, 8, 8) X(512, 32, 4, 1, 8, 8, 8) X(256, 16, 8, 1, 16, 16)
 
 template <int... Rs> constexpr bool sched_eq(const int *r, int nst) {
   constexpr int a[] = {Rs...};
