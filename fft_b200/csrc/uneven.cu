@@ -9,7 +9,9 @@
 // then every second phase, ...) and executed by k_persist, whose CTAs claim
 // (phase, tile) items from a counter; a phase waits, with a bounded spin, for
 // the phase it depends on.  The same phases can also be launched one kernel
-// each (the non-persistent mode, used to check the scheduler).
+// each (the per-phase mode: compiled-schedule kernels where they exist, the
+// length classes spread over four streams so independent classes overlap);
+// the autotuner picks the faster mode.
 #include <algorithm>
 #include <cstring>
 #include <map>
@@ -45,7 +47,11 @@ struct gofft_uneven {
   std::vector<Cls> cls;
   std::vector<PhaseDesc> ph[2];        // forward, inverse (user pointers as tags)
   std::vector<int> ph_level;
+  std::vector<int> ph_lane;            // per-phase launches: stream index (by class)
   std::vector<std::shared_ptr<DevProg>> ph_prog;
+  static constexpr int kLanes = 4;     // per-phase launches: classes spread over these streams
+  cudaStream_t lane[kLanes] = {};      // lane[0] unused (the caller's stream)
+  cudaEvent_t ev_fork = nullptr, ev_join[kLanes] = {};
   PhaseDesc *d_ph[2] = {nullptr, nullptr};
   PhaseDesc *h_pinned = nullptr;       // staging for pointer patches
   void *ws = nullptr;
@@ -69,6 +75,11 @@ struct gofft_uneven {
     if (h_pinned) cudaFreeHost(h_pinned);
     if (ws) cudaFree(ws);
     if (d_ctr) cudaFree(d_ctr);
+    for (int k = 1; k < kLanes; k++) {
+      if (lane[k]) cudaStreamDestroy(lane[k]);
+      if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
   }
 };
 
@@ -234,8 +245,18 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
   std::vector<int> lvl;
   std::vector<std::shared_ptr<DevProg>> progs;
   size_t wsoff = 0;
-  for (auto &c : u->cls)
-    if (int rc = add_class(u.get(), c, &wsoff, raw, lvl, progs)) return rc;
+  // classes spread over the per-phase lanes, largest first (round robin)
+  std::vector<size_t> by_size(u->cls.size());
+  for (size_t i = 0; i < by_size.size(); i++) by_size[i] = i;
+  std::stable_sort(by_size.begin(), by_size.end(), [&](size_t x, size_t y) {
+    return u->cls[x].n * (long long)u->cls[x].sig.size() > u->cls[y].n * (long long)u->cls[y].sig.size();
+  });
+  std::vector<int> cls_lane(u->cls.size()), raw_lane;
+  for (size_t r = 0; r < by_size.size(); r++) cls_lane[by_size[r]] = (int)(r % gofft_uneven::kLanes);
+  for (size_t ci = 0; ci < u->cls.size(); ci++) {
+    if (int rc = add_class(u.get(), u->cls[ci], &wsoff, raw, lvl, progs)) return rc;
+    raw_lane.resize(raw.size(), cls_lane[ci]);
+  }
   // order by level, keeping class order within a level; remap dependencies
   std::vector<int> order(raw.size());
   for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
@@ -252,6 +273,7 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
     first += p.ntiles;
     u->ph[0][i] = p;
     u->ph_level.push_back(lvl[order[i]]);
+    u->ph_lane.push_back(raw_lane[order[i]]);
     u->ph_prog.push_back(progs[order[i]]);
   }
   u->total = first;
@@ -316,6 +338,11 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
   for (int d = 0; d < 2; d++) GF_CK(cudaMalloc(&u->d_ph[d], u->nph * sizeof(PhaseDesc)));
   GF_CK(cudaMallocHost(&u->h_pinned, u->nph * sizeof(PhaseDesc)));
   GF_CK(cudaMalloc(&u->d_ctr, sizeof(unsigned long long) * (2 + (u->nph + 2) / 2)));
+  GF_CK(cudaEventCreateWithFlags(&u->ev_fork, cudaEventDisableTiming));
+  for (int k = 1; k < gofft_uneven::kLanes; k++) {
+    GF_CK(cudaStreamCreateWithFlags(&u->lane[k], cudaStreamNonBlocking));
+    GF_CK(cudaEventCreateWithFlags(&u->ev_join[k], cudaEventDisableTiming));
+  }
   *out = u.release();
   return GOFFT_OK;
 }
@@ -377,15 +404,27 @@ extern "C" int gofft_uneven_exec(gofft_uneven *u, const void *in, void *out, int
     GF_CK(cudaGetLastError());
     return GOFFT_OK;
   }
-  // one launch per phase, in phase order (dependencies are earlier phases)
+  // one launch per phase; a class's phases stay in order on its lane (its
+  // dependencies are earlier phases of the same class), classes on different
+  // lanes overlap; lanes fork from and join back into the caller's stream
+  GF_CK(cudaEventRecord(u->ev_fork, st));
+  for (int k = 1; k < gofft_uneven::kLanes; k++) GF_CK(cudaStreamWaitEvent(u->lane[k], u->ev_fork, 0));
   std::vector<PhaseDesc> t = u->ph[dir];
-  for (int i = 0; i < u->nph; i++) {
+  int rc = 0;
+  for (int i = 0; i < u->nph && !rc; i++) {
     PhaseDesc p = t[i];
     if (p.a.in.ptr == &g_in_tag) p.a.in.ptr = (void *)in;
     if (p.a.out.ptr == &g_out_tag) p.a.out.ptr = out;
     const bool conv = p.op == OP_RADER || p.op == OP_BLUE;
-    if (int rc = launch_line(p.op, *u->ph_prog[i], p.a, p.a.nlines, st, p.a.lpc, conv)) return rc;
+    const cudaStream_t s = u->ph_lane[i] ? u->lane[u->ph_lane[i]] : st;
+    rc = launch_line(p.op, *u->ph_prog[i], p.a, p.a.nlines, s, p.a.lpc, conv);
   }
+  for (int k = 1; k < gofft_uneven::kLanes; k++) {
+    cudaEventRecord(u->ev_join[k], u->lane[k]);
+    cudaStreamWaitEvent(st, u->ev_join[k], 0);
+  }
+  if (rc) return rc;
+  GF_CK(cudaGetLastError());
   return GOFFT_OK;
 }
 

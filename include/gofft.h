@@ -203,15 +203,18 @@ GOFFT_API int gofft_uneven_create(int precision, const int64_t *lengths, int64_t
                                   gofft_uneven **out);
 GOFFT_API int gofft_uneven_destroy(gofft_uneven *u);
 /* Forward or normalised inverse of every signal: one persistent kernel (plus a
- * counter reset) on `stream`; capturable in a CUDA graph once the batch has
- * run on the same buffers.  Errors of the device-side waits are reported by
+ * counter reset) on `stream`, or in the per-phase mode one launch per phase
+ * with the length classes spread over streams forked from and joined back
+ * into `stream`; capturable in a CUDA graph once the batch has run on the
+ * same buffers.  Errors of the device-side waits are reported by
  * gofft_uneven_status. */
 GOFFT_API int gofft_uneven_exec(gofft_uneven *u, const void *in, void *out, int inverse,
                                 gofft_stream stream);
 /* Synchronises and returns GOFFT_ETIMEOUT if a bounded wait of the last run
  * expired (its results are then invalid). */
 GOFFT_API int gofft_uneven_status(gofft_uneven *u);
-/* what = 0: persistent (1, default) or one launch per phase (0);
+/* what = 0: persistent (1, default unless the autotuner chose otherwise) or
+ * one launch per phase (0);
  * 1: poll limit of the device-side waits; 2: test hook that makes one wait
  * depend on work that never completes (to exercise the timeout path). */
 GOFFT_API int gofft_uneven_set(gofft_uneven *u, int what, int64_t value);
