@@ -83,6 +83,15 @@ SIGNATURES = {
     "gofft_set_lines_per_cta": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gofft_set_pipelined": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int]),
     "gofft_set_schedule": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int]),
+    "gofft_hamming": (ctypes.c_int, [_i64, _vp]),
+    "gofft_blackman": (ctypes.c_int, [_i64, _vp]),
+    "gofft_blackman_harris": (ctypes.c_int, [_i64, _vp]),
+    "gofft_bartlett": (ctypes.c_int, [_i64, _vp]),
+    "gofft_fftfreq": (ctypes.c_int, [_i64, ctypes.c_double, _vp]),
+    "gofft_rfftfreq": (ctypes.c_int, [_i64, ctypes.c_double, _vp]),
+    "gofft_window_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _i64, _vp, _vp]),
+    "gofft_spectrogram_window_device": (ctypes.c_int, [ctypes.c_int, _vp, _i64, _i64, _i64, ctypes.c_int,
+                                                       ctypes.c_double, _vp, _i64p, _vp]),
     "gofft_get_schedule": (ctypes.c_int, [ctypes.c_int, _i64]),
     "gofft_autotune": (_i64, [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _i64, ctypes.c_char_p, _i64]),
     "gofft_autotune_uneven": (_i64, [ctypes.c_int, _vp, _i64, ctypes.c_char_p, _i64]),

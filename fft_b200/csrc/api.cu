@@ -750,6 +750,103 @@ extern "C" int gofft_hann(int64_t n, double *out) {
   return GOFFT_OK;
 }
 
+// The other symmetric windows (window.go:29-100), on the host in FP64 exactly
+// as the reference writes them.
+static int cosine_window_host(int64_t n, const double *a, int na, double *out) {
+  if (n <= 0) return GOFFT_OK;
+  if (!out) return set_err(GOFFT_EINVAL, "null output");
+  if (n == 1) {
+    out[0] = 1;
+    return GOFFT_OK;
+  }
+  const double denom = (double)(n - 1);
+  for (int64_t k = 0; k < n; k++) {
+    double s = a[0], sign = -1.0;
+    for (int j = 1; j < na; j++) {
+      s += sign * a[j] * cos(2 * M_PI * (double)j * (double)k / denom);
+      sign = -sign;
+    }
+    out[k] = s;
+  }
+  return GOFFT_OK;
+}
+extern "C" int gofft_hamming(int64_t n, double *out) {
+  const double a[2] = {0.54, 0.46};
+  return cosine_window_host(n, a, 2, out);
+}
+extern "C" int gofft_blackman(int64_t n, double *out) {
+  const double a[3] = {0.42, 0.5, 0.08};
+  return cosine_window_host(n, a, 3, out);
+}
+extern "C" int gofft_blackman_harris(int64_t n, double *out) {
+  const double a[4] = {0.35875, 0.48829, 0.14128, 0.01168};
+  return cosine_window_host(n, a, 4, out);
+}
+extern "C" int gofft_bartlett(int64_t n, double *out) {
+  if (n <= 0) return GOFFT_OK;
+  if (!out) return set_err(GOFFT_EINVAL, "null output");
+  if (n == 1) {
+    out[0] = 1;
+    return GOFFT_OK;
+  }
+  const double denom = (double)(n - 1), half = denom / 2;
+  for (int64_t k = 0; k < n; k++) out[k] = (2 / denom) * (half - fabs((double)k - half));
+  return GOFFT_OK;
+}
+
+// FFTFreq / RFFTFreq (freq.go:17-56).
+extern "C" int gofft_fftfreq(int64_t n, double d, double *out) {
+  if (n <= 0) return GOFFT_OK;
+  if (!out) return set_err(GOFFT_EINVAL, "null output");
+  const double val = 1.0 / (d * (double)n);
+  const int64_t half = (n - 1) / 2;
+  for (int64_t i = 0; i <= half; i++) out[i] = (double)i * val;
+  int64_t j = -(n / 2);
+  for (int64_t i = half + 1; i < n; i++, j++) out[i] = (double)j * val;
+  return GOFFT_OK;
+}
+extern "C" int gofft_rfftfreq(int64_t n, double d, double *out) {
+  if (n <= 0) return GOFFT_OK;
+  if (!out) return set_err(GOFFT_EINVAL, "null output");
+  const double val = 1.0 / (d * (double)n);
+  for (int64_t i = 0; i < n / 2 + 1; i++) out[i] = (double)i * val;
+  return GOFFT_OK;
+}
+
+// Device windows, generated once per (device, precision, kind, length) and
+// kept for the process: the spectrogram's fused first stage reads them.
+static const void *device_window(int prec, int kind, int64_t n, cudaStream_t st) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int64_t>, void *> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_tuple(dev, prec, kind, n);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  void *w = nullptr;
+  const int rb = prec == F64 ? 8 : 4;
+  if (cudaMalloc(&w, (size_t)n * rb) != cudaSuccess) {
+    set_err(GOFFT_ENOMEM, "window buffer");
+    return nullptr;
+  }
+  if (gen_window(w, rb, n, kind, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+    cudaFree(w);
+    set_err(GOFFT_ECUDA, "window generation failed");
+    return nullptr;
+  }
+  cache[key] = w;
+  return w;
+}
+
+extern "C" int gofft_window_device(int precision, int kind, int64_t n, void *out, gofft_stream stream) {
+  if (precision < 0 || precision > 2 || kind < 0 || kind > 4) return set_err(GOFFT_EINVAL, "bad window arguments");
+  if (n <= 0) return GOFFT_OK;
+  if (!out) return set_err(GOFFT_EINVAL, "null output");
+  GF_CK(gen_window(out, precision == F64 ? 8 : 4, n, kind, (cudaStream_t)stream));
+  return GOFFT_OK;
+}
+
 // Spectrogram frames on device buffers (freq.go:107-127 for even segments).
 static int spectro_dev(int prec, const void *x, int64_t nx, int64_t seg, int64_t overlap, const void *win,
                        double d, void *out, int64_t frames, cudaStream_t st) {
@@ -787,6 +884,16 @@ extern "C" int gofft_spectrogram_device(int precision, const void *x, int64_t nx
   if (nframes) *nframes = frames;
   if (!out) return GOFFT_OK;
   return spectro_dev(precision, x, nx, segment, overlap, window, d, out, frames, (cudaStream_t)stream);
+}
+
+extern "C" int gofft_spectrogram_window_device(int precision, const void *x, int64_t nx, int64_t segment,
+                                               int64_t overlap, int window_kind, double d, void *out,
+                                               int64_t *nframes, gofft_stream stream) {
+  if (window_kind < 0 || window_kind > 4) return set_err(GOFFT_EINVAL, "bad window kind");
+  if (segment <= 0) return set_err(GOFFT_EINVAL, "fft: segment length must be positive");
+  const void *w = device_window(precision, window_kind, segment, (cudaStream_t)stream);
+  if (!w) return GOFFT_ECUDA;
+  return gofft_spectrogram_device(precision, x, nx, segment, overlap, w, d, out, nframes, stream);
 }
 
 // PSD (freq.go:69-90) of one host signal.

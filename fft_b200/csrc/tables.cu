@@ -86,4 +86,44 @@ cudaError_t gen_blue_kernel(double2 *b, const double2 *w, long long n, long long
   return cudaGetLastError();
 }
 
+// Symmetric windows (window.go:20-100) in FP64 on the device, stored in the
+// output's precision.  Cosine windows w[k] = sum_j (-1)^j a_j cos(2 pi j k /
+// (n-1)) take each angle from the exact integer residue j k mod (n-1), so
+// cospi's argument is reduced without rounding; Bartlett is the triangle
+// (2/(n-1)) ((n-1)/2 - |k - (n-1)/2|).  kind: 0 Hann, 1 Hamming, 2 Blackman,
+// 3 Blackman-Harris, 4 Bartlett.
+template <class R>
+__global__ void k_gen_window(R *w, long long n, int kind) {
+  const double a[4][4] = {{0.5, 0.5, 0, 0}, {0.54, 0.46, 0, 0}, {0.42, 0.5, 0.08, 0},
+                          {0.35875, 0.48829, 0.14128, 0.01168}};
+  const int na = kind == 2 ? 3 : (kind == 3 ? 4 : 2);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    double v;
+    if (n == 1) {
+      v = 1.0;
+    } else if (kind == 4) {
+      const double denom = (double)(n - 1), half = denom / 2;
+      v = (2 / denom) * (half - fabs((double)k - half));
+    } else {
+      v = a[kind][0];
+      double sign = -1.0;
+      for (int j = 1; j < na; j++) {
+        const long long e = ((long long)j * k) % (n - 1);
+        v += sign * a[kind][j] * cospi(2.0 * (double)e / (double)(n - 1));
+        sign = -sign;
+      }
+    }
+    w[k] = (R)v;
+  }
+}
+
+cudaError_t gen_window(void *w, int prec_bytes, long long n, int kind, cudaStream_t st) {
+  if (prec_bytes == 8)
+    k_gen_window<double><<<tb_blocks(n), 256, 0, st>>>((double *)w, n, kind);
+  else
+    k_gen_window<float><<<tb_blocks(n), 256, 0, st>>>((float *)w, n, kind);
+  return cudaGetLastError();
+}
+
 }  // namespace gf

@@ -214,6 +214,36 @@ def spectrogram(x, segment, overlap, window, d, precision="f64", stream=None):
     return out
 
 
+WINDOWS = {"hann": 0, "hamming": 1, "blackman": 2, "blackmanharris": 3, "bartlett": 4}
+
+
+def window(kind, n, precision="f64", stream=None):
+    """A symmetric window (window.go:20-100) generated on the device."""
+    prec = PRECISIONS[precision]
+    out = torch.empty(int(n), dtype=RDT[prec], device="cuda")
+    if n > 0:
+        check(lib().gofft_window_device(prec, WINDOWS[kind], int(n), ctypes.c_void_p(out.data_ptr()),
+                                        _stream(stream)))
+    return out
+
+
+def spectrogram_window(x, segment, overlap, kind, d, precision="f64", stream=None):
+    """Fused spectrogram with a device-generated window of `kind`."""
+    prec = PRECISIONS[precision]
+    _need(x, RDT[prec], "x")
+    nf = ctypes.c_int64()
+    check(lib().gofft_spectrogram_window_device(prec, ctypes.c_void_p(x.data_ptr()), x.numel(), int(segment),
+                                                int(overlap), WINDOWS[kind], float(d), None, ctypes.byref(nf),
+                                                _stream(stream)))
+    out = torch.empty((nf.value, int(segment) // 2 + 1), dtype=RDT[prec], device=x.device)
+    if nf.value:
+        check(lib().gofft_spectrogram_window_device(prec, ctypes.c_void_p(x.data_ptr()), x.numel(), int(segment),
+                                                    int(overlap), WINDOWS[kind], float(d),
+                                                    ctypes.c_void_p(out.data_ptr()), ctypes.byref(nf),
+                                                    _stream(stream)))
+    return out
+
+
 class UnevenBatch:
     """Complex transforms of different lengths in one persistent launch
     (gofft_uneven_*).  Signals are packed back to back in one tensor unless

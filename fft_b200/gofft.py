@@ -245,6 +245,52 @@ def Hann(n):
     return out
 
 
+def _window(fn, n):
+    if n <= 0:
+        return np.zeros(0)
+    out = np.zeros(n)
+    _call(fn(int(n), _ptr(out)))
+    return out
+
+
+def Hamming(n):
+    """window.go:29-31"""
+    return _window(lib().gofft_hamming, n)
+
+
+def Blackman(n):
+    """window.go:38-40"""
+    return _window(lib().gofft_blackman, n)
+
+
+def BlackmanHarris(n):
+    """window.go:48-50"""
+    return _window(lib().gofft_blackman_harris, n)
+
+
+def Bartlett(n):
+    """window.go:86-100"""
+    return _window(lib().gofft_bartlett, n)
+
+
+def FFTFreq(n, d):
+    """freq.go:17-37"""
+    if n <= 0:
+        return np.zeros(0)
+    out = np.zeros(n)
+    _call(lib().gofft_fftfreq(int(n), float(d), _ptr(out)))
+    return out
+
+
+def RFFTFreq(n, d):
+    """freq.go:46-56"""
+    if n <= 0:
+        return np.zeros(0)
+    out = np.zeros(n // 2 + 1)
+    _call(lib().gofft_rfftfreq(int(n), float(d), _ptr(out)))
+    return out
+
+
 def PSD(x, d):
     """freq.go:69-90"""
     x = _f64(x)

@@ -115,6 +115,16 @@ GOFFT_API int gofft_irfft2(const double *data, int64_t len, int64_t rows, int64_
 
 /* Hann (window.go:20-22): symmetric window of length n (n <= 0: none). */
 GOFFT_API int gofft_hann(int64_t n, double *out);
+/* Hamming, Blackman, BlackmanHarris, Bartlett (window.go:29-100): symmetric
+ * windows of length n (n <= 0: none, n == 1: {1}). */
+GOFFT_API int gofft_hamming(int64_t n, double *out);
+GOFFT_API int gofft_blackman(int64_t n, double *out);
+GOFFT_API int gofft_blackman_harris(int64_t n, double *out);
+GOFFT_API int gofft_bartlett(int64_t n, double *out);
+/* FFTFreq (freq.go:17-37): n bin frequencies for spacing d; RFFTFreq
+ * (freq.go:46-56): n/2+1 of them (n <= 0: none). */
+GOFFT_API int gofft_fftfreq(int64_t n, double d, double *out);
+GOFFT_API int gofft_rfftfreq(int64_t n, double d, double *out);
 /* PSD (freq.go:69-90): one-sided density of n reals at spacing d -> n/2+1. */
 GOFFT_API int gofft_psd(const double *x, int64_t n, double d, double *out);
 /* Spectrogram (freq.go:107-127): frames of `segment` samples every
@@ -188,6 +198,18 @@ GOFFT_API int64_t gofft_plan_table(const gofft_plan *p, int which, int64_t *out,
 GOFFT_API int gofft_spectrogram_device(int precision, const void *x, int64_t nx, int64_t segment,
                              int64_t overlap, const void *window, double d, void *out,
                              int64_t *nframes, gofft_stream stream);
+
+/* A window (kind 0 Hann, 1 Hamming, 2 Blackman, 3 Blackman-Harris,
+ * 4 Bartlett; window.go:20-100) of n samples generated on the device in FP64
+ * (angles from exact integer residues) and stored in the precision's real
+ * type.  No reference counterpart (the reference builds windows on the host). */
+GOFFT_API int gofft_window_device(int precision, int kind, int64_t n, void *out, gofft_stream stream);
+/* gofft_spectrogram_device with a window of `window_kind` generated on the
+ * device (once per kind, length and precision, then kept) instead of a
+ * caller's buffer. */
+GOFFT_API int gofft_spectrogram_window_device(int precision, const void *x, int64_t nx, int64_t segment,
+                                              int64_t overlap, int window_kind, double d, void *out,
+                                              int64_t *nframes, gofft_stream stream);
 
 /* ------------------------------------------------------------------------ */
 /* 2b. Uneven batches (no counterpart in the reference, whose batches are a   */

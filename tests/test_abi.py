@@ -116,3 +116,28 @@ def test_wisdom_roundtrip():
     tune.forget_wisdom()
     got = json.loads(tune.export_wisdom())
     assert got["schedule"] == [] and got["lpc"] == [] and got["pipe"] == [] and got["uneven"] == []
+
+
+def test_host_windows_and_frequencies():
+    """The reference-facing windows and bin frequencies (host code, no GPU):
+    FFTFreq/RFFTFreq equal numpy's exactly (freq.go:17-56 promises it); the
+    windows agree with numpy / scipy and with the oracle's cosine window to
+    rounding."""
+    import scipy.signal
+    from fft_b200 import gofft as G
+    from oracle import oracle as O
+    for n in [1, 2, 7, 8, 1000, 1001]:
+        for d in [1.0, 0.1, 3.7]:
+            np.testing.assert_array_equal(G.FFTFreq(n, d), np.fft.fftfreq(n, d))
+            np.testing.assert_array_equal(G.RFFTFreq(n, d), np.fft.rfftfreq(n, d))
+        assert np.max(np.abs(G.Hamming(n) - np.hamming(n))) < 1e-15
+        assert np.max(np.abs(G.Blackman(n) - np.blackman(n))) < 1e-15
+        assert np.max(np.abs(G.Bartlett(n) - np.bartlett(n))) < 1e-15
+        bh = scipy.signal.windows.blackmanharris(n, sym=True)
+        assert np.max(np.abs(G.BlackmanHarris(n) - bh)) < 1e-15
+        np.testing.assert_array_equal(G.Hamming(n), O.cosine_window(n, [0.54, 0.46]))
+        np.testing.assert_array_equal(G.Blackman(n), O.cosine_window(n, [0.42, 0.5, 0.08]))
+    for f in (G.FFTFreq, G.RFFTFreq):
+        assert f(0, 1.0).size == 0 and f(-3, 1.0).size == 0
+    for f in (G.Hamming, G.Blackman, G.BlackmanHarris, G.Bartlett):
+        assert f(0).size == 0 and list(f(1)) == [1.0]
