@@ -89,6 +89,11 @@ cudaError_t gen_rader_kernel(double2 *b, const int *perm, long long p, long long
                              cudaStream_t st);
 cudaError_t gen_chirp(long long *jj, double2 *w, long long n, cudaStream_t st);
 cudaError_t gen_blue_kernel(double2 *b, const double2 *w, long long n, long long m, cudaStream_t st);
+// The persistent multi-phase kernel (k_persist) of each precision.
+const void *persist_kernel_f64();
+const void *persist_kernel_f32();
+const void *persist_kernel_f32c();
+
 // Window of `kind` (0 Hann, 1 Hamming, 2 Blackman, 3 Blackman-Harris,
 // 4 Bartlett), n samples of prec_bytes (8 or 4) each.
 cudaError_t gen_window(void *w, int prec_bytes, long long n, int kind, cudaStream_t st);

@@ -384,13 +384,15 @@ template <int N, int T, int R, int... Rs> constexpr int ct_maxe_r() {
 // offsets.
 template <int STEP, class C> GF_DEV C &slot(C *b, int i) { return b[spad(i) * STEP]; }
 
-template <class P, class Op, int N, int T, int NS, int R, int E, bool FG, bool TG, int STEP>
+// GUARD: some threads of the block sit out the butterflies (c.t beyond the
+// line); every thread still reaches the barriers.
+template <class P, class Op, int N, int T, int NS, int R, int E, bool FG, bool TG, int STEP, bool GUARD>
 GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &a, const LineCtx &c,
                      const typename P::tw_t *tw, const float2 *twh, bool cj) {
   using C = typename P::cpx;
   constexpr int NB = N / R;
   constexpr int PER = (NB + T - 1) / T;
-  constexpr bool EXACT = (NB % T) == 0;
+  constexpr bool EXACT = (NB % T) == 0 && !GUARD;
 #pragma unroll
   for (int b = 0; b < PER; b++) {
     const int j = c.t + b * T;
@@ -449,8 +451,8 @@ GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &
   if constexpr (!TG) __syncthreads();
 }
 
-template <class P, class Op, int N, int T, int NS, int TO, int E, bool CAN_FG, bool CAN_TG, int STEP, int R,
-          int... Rs>
+template <class P, class Op, int N, int T, int NS, int TO, int E, bool CAN_FG, bool CAN_TG, int STEP, bool GUARD,
+          int R, int... Rs>
 GF_DEV void stages_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &a, const LineCtx &c,
                       bool cj_first, bool fg, bool tg) {
   using TW = typename P::tw_t;
@@ -462,32 +464,32 @@ GF_DEV void stages_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs 
   constexpr bool F_OK = FIRST && CAN_FG;
   constexpr bool T_OK = LAST && CAN_TG;
   if constexpr (F_OK && T_OK) {
-    if (fg && tg) stage_ct<P, Op, N, T, NS, R, E, true, true, STEP>(v, sb, a, c, tw, twh, cj);
-    else if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP>(v, sb, a, c, tw, twh, cj);
-    else if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP>(v, sb, a, c, tw, twh, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, twh, cj);
+    if (fg && tg) stage_ct<P, Op, N, T, NS, R, E, true, true, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
+    else if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
+    else if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
   } else if constexpr (F_OK) {
-    if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP>(v, sb, a, c, tw, twh, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, twh, cj);
+    if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
   } else if constexpr (T_OK) {
-    if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP>(v, sb, a, c, tw, twh, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, twh, cj);
+    if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
   } else {
-    stage_ct<P, Op, N, T, NS, R, E, false, false, STEP>(v, sb, a, c, tw, twh, cj);
+    stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
   }
   if constexpr (!LAST)
-    stages_ct<P, Op, N, T, NS * R, TO + NS * (R - 1), E, CAN_FG, CAN_TG, STEP, Rs...>(v, sb, a, c, cj_first, fg,
-                                                                                      tg);
+    stages_ct<P, Op, N, T, NS * R, TO + NS * (R - 1), E, CAN_FG, CAN_TG, STEP, GUARD, Rs...>(v, sb, a, c, cj_first,
+                                                                                             fg, tg);
 }
 
 // Runs the compiled schedule on the line at shared-memory base sb; STEP is
 // the element step of the layout (1: row layout, LPC: column layout).
-template <class P, class Op, int N, int T, bool CAN_FG, bool CAN_TG, int STEP, int... Rs>
+template <class P, class Op, int N, int T, bool CAN_FG, bool CAN_TG, int STEP, bool GUARD = false, int... Rs>
 GF_DEV void run_stages_ct(Sched<Rs...>, typename P::cpx *sb, const KArgs &a, const LineCtx &c, bool cj_first,
                           bool fg, bool tg) {
   constexpr int E = ct_maxe_r<N, T, Rs...>();
   typename P::cpx v[E];
-  stages_ct<P, Op, N, T, 1, 0, E, CAN_FG, CAN_TG, STEP, Rs...>(v, sb, a, c, cj_first, fg, tg);
+  stages_ct<P, Op, N, T, 1, 0, E, CAN_FG, CAN_TG, STEP, GUARD, Rs...>(v, sb, a, c, cj_first, fg, tg);
 }
 
 }  // namespace gf

@@ -131,6 +131,29 @@ template <class P, int GROUP> KFn pick_ct(int n, int T, int lpc, int op, const i
   return nullptr;
 }
 
+// Compiled schedules the persistent (uneven-batch) kernel runs: the default
+// schedule of every power-of-two length up to 4096 at its row- and
+// column-layout lines per CTA.
+#define GF_PERSIST_LIST(X)                                                               \
+  X(64, 4, 64, 8, 8) X(64, 4, 128, 8, 8) X(128, 8, 32, 16, 8) X(128, 8, 64, 16, 8)     \
+  X(256, 16, 16, 16, 16) X(256, 16, 32, 16, 16) X(512, 32, 8, 8, 8, 8)                \
+  X(512, 32, 16, 8, 8, 8) X(1024, 64, 4, 16, 8, 8) X(1024, 64, 8, 16, 8, 8)           \
+  X(2048, 128, 2, 16, 16, 8) X(2048, 128, 4, 16, 16, 8) X(4096, 256, 1, 16, 16, 16)   \
+  X(4096, 256, 2, 16, 16, 16)
+
+template <class P> GF_DEV bool persist_ct(const KArgs &a, int op, long long tile, bool active) {
+  const int n = a.lp.n, T = a.lp.T, L = a.lpc;
+#define GF_PX(N, TT, LL, ...)                                                                   \
+  if (n == N && T == TT && L == LL && sched_eq<__VA_ARGS__>(a.lp.radix, a.lp.nst)) {           \
+    if (op == OP_C2C) persist_ct_body<P, N, TT, LL, OpC2C, Sched<__VA_ARGS__>>(a, tile, active); \
+    else persist_ct_body<P, N, TT, LL, OpC2CTwiddle, Sched<__VA_ARGS__>>(a, tile, active);      \
+    return true;                                                                               \
+  }
+  GF_PERSIST_LIST(GF_PX)
+#undef GF_PX
+  return false;
+}
+
 static inline int ew_blocks(long long total) {
   long long b = (total + 255) / 256;
   if (b > 148 * 32) b = 148 * 32;
@@ -142,6 +165,7 @@ static inline int ew_blocks(long long total) {
 
 #define GF_DEFINE_PREC(P, SUFFIX)                                                              \
   namespace gf {                                                                               \
+  const void *persist_kernel_##SUFFIX() { return (const void *)k_persist<P>; }                \
   namespace prec_##SUFFIX {                                                                    \
   using C = P::cpx;                                                                            \
   using SP = P::sp_t;                                                                          \

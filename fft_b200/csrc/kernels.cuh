@@ -75,16 +75,64 @@ struct PhaseDesc {
   long long first;   // number of the phase's first item
 };
 
+// A persistent kernel's tile on a compiled schedule (complex group-0 ops with
+// the tile prologue and epilogue; uneven phases have no direct stages).
+// Threads past the phase's LPC*T threads take part in the barriers only.  Not
+// inlined: each body keeps its own register allocation.
+template <class P, int N, int T, int LPC, class Op, class S>
+__device__ __noinline__ void persist_ct_body(const KArgs &a, long long tile, bool active) {
+  using C = typename P::cpx;
+  const long long line0 = tile * LPC;
+  LineCtx c;
+  if (!active) {
+    c.l = 0;
+    c.t = 1 << 29;  // no butterflies
+  } else if (a.flags & GF_COLMAP) {
+    c.l = threadIdx.x % LPC;
+    c.t = threadIdx.x / LPC;
+  } else {
+    c.l = threadIdx.x / T;
+    c.t = threadIdx.x % T;
+  }
+  c.line = line0 + c.l;
+  c.valid = active && c.line < a.nlines;
+  c.ioff = 0;
+  c.ooff = 0;
+  Op::template load<P>(a, line0);
+  cp_async_wait_all();
+  __syncthreads();
+  Op::template prep<P>(a, line0);
+  C *sb = line_view<C>(a, c.l).b;
+  if (a.flags & GF_COLMAP)
+    run_stages_ct<P, Op, N, T, false, false, LPC, true>(S{}, sb, a, c, Op::first_conj(a), false, false);
+  else
+    run_stages_ct<P, Op, N, T, false, false, 1, true>(S{}, sb, a, c, Op::first_conj(a), false, false);
+  Op::template store<P>(a, line0);
+}
+
+// Runs the tile on a compiled schedule when one matches the phase (defined
+// beside the list of compiled schedules); false otherwise.
+template <class P> GF_DEV bool persist_ct(const KArgs &a, int op, long long tile, bool active);
+
+// One op's run-time-schedule body as its own function (not inlined: the
+// persistent kernel calls one per phase, and inlining all of them into one
+// body made the register allocator spill).
+template <class P, class Op>
+__device__ __noinline__ void persist_line_body(const KArgs &a, long long tile, bool active) {
+  line_body<P, 16, Op>(a, tile, active);
+}
+
 template <class P>
 GF_DEV void phase_dispatch(const KArgs &a, int op, long long tile, bool active) {
+  if ((op == OP_C2C || op == OP_C2C_TW) && persist_ct<P>(a, op, tile, active)) return;
   switch (op) {
-    case OP_C2C: line_body<P, 16, OpC2C>(a, tile, active); break;
-    case OP_C2C_TW: line_body<P, 16, OpC2CTwiddle>(a, tile, active); break;
-    case OP_RADER: line_body<P, 16, OpRader>(a, tile, active); break;
-    case OP_BLUE: line_body<P, 16, OpBluestein>(a, tile, active); break;
-    case OP_RADER_FS1: line_body<P, 16, OpRaderFS1>(a, tile, active); break;
-    case OP_RADER_FS2: line_body<P, 16, OpRaderFS2>(a, tile, active); break;
-    case OP_RADER_FS4: line_body<P, 16, OpRaderFS4>(a, tile, active); break;
+    case OP_C2C: persist_line_body<P, OpC2C>(a, tile, active); break;
+    case OP_C2C_TW: persist_line_body<P, OpC2CTwiddle>(a, tile, active); break;
+    case OP_RADER: persist_line_body<P, OpRader>(a, tile, active); break;
+    case OP_BLUE: persist_line_body<P, OpBluestein>(a, tile, active); break;
+    case OP_RADER_FS1: persist_line_body<P, OpRaderFS1>(a, tile, active); break;
+    case OP_RADER_FS2: persist_line_body<P, OpRaderFS2>(a, tile, active); break;
+    case OP_RADER_FS4: persist_line_body<P, OpRaderFS4>(a, tile, active); break;
     default: break;
   }
 }

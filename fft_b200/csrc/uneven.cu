@@ -83,6 +83,13 @@ struct gofft_uneven {
   }
 };
 
+// The persistent kernel of a precision (instantiated with the compiled
+// schedules it dispatches to, in the precision's own translation unit).
+using PersistFn = void (*)(const PhaseDesc *, int, long long, unsigned long long *, int *, int *, long long);
+static const void *persist_fn(int prec) {
+  return prec == F64 ? persist_kernel_f64() : prec == F32 ? persist_kernel_f32() : persist_kernel_f32c();
+}
+
 static int *done_ptr(gofft_uneven *u) { return reinterpret_cast<int *>(u->d_ctr + 1); }
 static int *err_ptr(gofft_uneven *u) { return done_ptr(u) + u->nph; }
 
@@ -326,9 +333,7 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
                                     (conv ? 2 * p.a.lpc * csize(precision) : 0));
   }
   u->block = (u->block + 31) / 32 * 32;
-  const void *kp = precision == F64 ? (const void *)k_persist<PrecF64>
-                   : precision == F32 ? (const void *)k_persist<PrecF32>
-                                      : (const void *)k_persist<PrecF32C>;
+  const void *kp = persist_fn(precision);
   if (u->smem > 48 * 1024) GF_CK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u->smem));
   int per_sm = 0, sms = 0;
   GF_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kp, u->block, u->smem));
@@ -387,20 +392,9 @@ extern "C" int gofft_uneven_exec(gofft_uneven *u, const void *in, void *out, int
   if (u->persistent) {
     GF_CK(cudaMemsetAsync(u->d_ctr, 0, sizeof(unsigned long long) * (2 + (u->nph + 2) / 2), st));
     count_launch();
-    switch (u->prec) {
-      case F64:
-        k_persist<PrecF64><<<u->grid, u->block, u->smem, st>>>(u->d_ph[dir], u->nph, u->total, u->d_ctr,
-                                                                done_ptr(u), err_ptr(u), u->spin_limit);
-        break;
-      case F32:
-        k_persist<PrecF32><<<u->grid, u->block, u->smem, st>>>(u->d_ph[dir], u->nph, u->total, u->d_ctr,
-                                                                done_ptr(u), err_ptr(u), u->spin_limit);
-        break;
-      default:
-        k_persist<PrecF32C><<<u->grid, u->block, u->smem, st>>>(u->d_ph[dir], u->nph, u->total, u->d_ctr,
-                                                                 done_ptr(u), err_ptr(u), u->spin_limit);
-        break;
-    }
+    const PersistFn fn = (PersistFn)persist_fn(u->prec);
+    fn<<<u->grid, u->block, u->smem, st>>>(u->d_ph[dir], u->nph, u->total, u->d_ctr, done_ptr(u), err_ptr(u),
+                                           u->spin_limit);
     GF_CK(cudaGetLastError());
     return GOFFT_OK;
   }
