@@ -47,7 +47,7 @@ def algo_bytes(prec_bytes):
 # of a launch over whole images (dram__bytes_read.sum + dram__bytes_write.sum,
 # caches flushed before the launch), divided by the images it covered; and
 # how many passes of each kernel a round trip makes over every image.
-DRAM_PER_IMAGE = {"c2c/n=1024/prec=0": 8424640, "r2c_packed/n=512/prec=0": 8482370}
+DRAM_PER_IMAGE = {"c2c/n=1024/prec=0": 8425280, "r2c_packed/n=512/prec=0": 8406720}
 PASSES = {"c2c": 2, "r2c_packed": 1, "c2r_packed": 1}
 
 
@@ -304,14 +304,30 @@ def extra_workloads(peak):
         for i in range(K):
             p1.c2c(xs[i], out=ys[i])
             p1.c2c(ys[i], out=xs[i], inverse=True)
-    ms = _events_ms(torch, c1, 5) / K
-    hot = _events_ms(torch, lambda: (p1.c2c(xs[0], out=ys[0]), p1.c2c(ys[0], out=xs[0], inverse=True)), 50)
+    ms_eager = _events_ms(torch, c1, 5) / K
+    # the same 2 x 64 calls captured once and replayed: device time without
+    # the host's per-call overhead (the eager figure above includes it)
+    s1 = torch.cuda.Stream()
+    with torch.cuda.stream(s1):
+        with Graph(s1) as g1:
+            for i in range(K):
+                p1.c2c(xs[i], out=ys[i], stream=s1)
+                p1.c2c(ys[i], out=xs[i], inverse=True, stream=s1)
+        ms = _events_ms(torch, g1.replay, 5) / K
+        with Graph(s1) as g0:
+            p1.c2c(xs[0], out=ys[0], stream=s1)
+            p1.c2c(ys[0], out=xs[0], inverse=True, stream=s1)
+        hot = _events_ms(torch, g0.replay, 50)
+    torch.cuda.synchronize()
+    del g1, g0
     p1.c2c(torch.from_numpy(x1).cuda(), out=ys[0])
     rel = _rel(ys[0][:16].cpu().numpy(), O.batch_fft(x1[:16]))
     gfl = 2 * 256 * 5 * 1024 * 10 / (ms / 1e3) / 1e9
-    res["c1_fft_256x1024_c128"] = line(ms, 16777216, {"l2_hot_ms": round(hot, 4), "gflops_5nlogn": round(gfl, 1),
+    res["c1_fft_256x1024_c128"] = line(ms, 16777216, {"l2_hot_ms": round(hot, 4), "eager_calls_ms": round(ms_eager, 4),
+                                                      "gflops_5nlogn": round(gfl, 1),
                                                       "rel_l2_vs_oracle": rel, "dtype": "f64",
-                                                      "note": "forward+inverse, rotation over 64 buffer sets"})
+                                                      "note": "forward+inverse, rotation over 64 buffer sets, "
+                                                              "CUDA-graph replay"})
     del xs, ys
 
     # C3: 4096 complex64 signals, lengths uniform over 8 lengths, seed 2
@@ -325,13 +341,16 @@ def extra_workloads(peak):
     yout = torch.empty_like(xin)
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
+        # the autotuner's pick: one persistent launch or one launch per phase
+        picked = "persistent launch" if u.describe()["persistent"] else "one launch per phase"
         ms = _events_ms(torch, lambda: u(xin, out=yout, stream=s), 20)
         with Graph(s) as gr:
             u(xin, out=yout, stream=s)
         msg = _events_ms(torch, gr.replay, 20)
+        u.set(0, 1)  # one persistent launch over all phases
+        mspl = _events_ms(torch, lambda: u(xin, out=yout, stream=s), 20)
         u.set(0, 0)  # one launch per phase (compiled-schedule kernels where they exist)
         mspp = _events_ms(torch, lambda: u(xin, out=yout, stream=s), 20)
-        u.set(0, 1)
         u(xin, out=yout, stream=s)
     torch.cuda.synchronize()
     got = yout.cpu().numpy()
@@ -339,9 +358,10 @@ def extra_workloads(peak):
     pick = [int(i) for i in np.random.default_rng(9).choice(len(lens), 24, replace=False)]
     rel = max(_rel(got[offs[i]:offs[i + 1]], O.fft(flat[offs[i]:offs[i + 1]].astype(np.complex128))) for i in pick)
     res["c3_uneven_4096_c64"] = line(ms, tot * 16, {"graph_replay_ms": round(msg, 4),
+                                                    "persistent_launch_ms": round(mspl, 4),
                                                     "per_phase_launches_ms": round(mspp, 4), "points": tot,
                                                     "status": u.status(), "max_rel_l2_24_signals": rel,
-                                                    "dtype": "f32mixed", "note": "forward, one persistent launch"})
+                                                    "dtype": "f32mixed", "note": "forward, " + picked})
     del u, xin, yout
 
     # C4: FFTN 256^3 complex64 (unit-variance complex Gaussian, seed 3)

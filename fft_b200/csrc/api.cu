@@ -64,6 +64,20 @@ static long long env_ll(const char *name, long long dflt) {
   return atoll(v);
 }
 
+// Items per L2 block for `units` items in at least `want` blocks: the
+// smallest block count from `want` up whose equal-as-possible blocks come out
+// even (when there are items for it), so the two lanes get the same number of
+// blocks instead of one lane running the last block alone.
+static long long lane_chunk(long long units, long long want) {
+  const long long first = (units + want - 1) / want;
+  if (want <= 1) return first;
+  for (long long nb = want; nb <= units; nb++) {
+    const long long chunk = (units + nb - 1) / nb;
+    if (((units + chunk - 1) / chunk) % 2 == 0) return chunk;
+  }
+  return first;
+}
+
 // Extent (elements) of `batch` lines of `len` elements at (dist, stride).
 static long long extent(long long batch, long long dist, long long len, long long stride) {
   if (batch <= 0 || len <= 0) return 0;
@@ -154,7 +168,7 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
           std::max<long long>(1, std::min<long long>(units, budget / (plane * (long long)csize(precision))));
       const long long nblocks = (units + cmax - 1) / cmax;
       if (nblocks > 1 && env_ll("GOFFT_LANES", 2) >= 2) {
-        p->nplane_blocks = (units + nblocks - 1) / nblocks;
+        p->nplane_blocks = lane_chunk(units, nblocks);
         p->nlanes = 2;
       }
     }
@@ -172,10 +186,11 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       const long long per = p->shape[0] * rc * (long long)csize(precision);
       const long long cmax = std::max<long long>(1, std::min<long long>(batch, budget / std::max<long long>(1, per)));
       const long long nblocks = (batch + cmax - 1) / cmax;
-      p->chunk = (batch + nblocks - 1) / nblocks;  // balanced blocks
       // two lanes: block i+1's passes overlap block i's (each pass alone
       // ramps up and drains; the other lane fills those gaps)
-      if (nblocks > 1 && env_ll("GOFFT_LANES", 2) >= 2) p->nlanes = 2;
+      const bool lanes = nblocks > 1 && env_ll("GOFFT_LANES", 2) >= 2;
+      p->chunk = lanes ? lane_chunk(batch, nblocks) : (batch + nblocks - 1) / nblocks;  // balanced blocks
+      if (lanes) p->nlanes = 2;
     }
   }
   if (int rc2 = plan_ws(p.get())) return rc2;

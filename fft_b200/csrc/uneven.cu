@@ -451,7 +451,7 @@ extern "C" int64_t gofft_uneven_describe(const gofft_uneven *u, char *buf, int64
   std::ostringstream o;
   o << "{\"count\":" << u->count << ",\"precision\":" << u->prec << ",\"phases\":" << u->nph
     << ",\"items\":" << u->total << ",\"grid\":" << u->grid << ",\"block\":" << u->block << ",\"smem\":" << u->smem
-    << ",\"workspace\":" << u->ws_bytes << ",\"classes\":[";
+    << ",\"workspace\":" << u->ws_bytes << ",\"persistent\":" << u->persistent << ",\"classes\":[";
   for (size_t i = 0; i < u->cls.size(); i++)
     o << (i ? "," : "") << "{\"n\":" << u->cls[i].n << ",\"count\":" << u->cls[i].sig.size()
       << ",\"exec\":" << u->cls[i].ex->describe() << "}";

@@ -49,6 +49,7 @@ def test_uneven_c3_lengths(prec, persistent):
     check_all(lengths, z.cpu().numpy(), parts, prec, inverse=True)
     d = u.describe()
     assert d["items"] > 0 and len(d["classes"]) == len(set(lengths))
+    assert d["persistent"] == persistent
 
 
 def test_uneven_inplace_and_offsets():
