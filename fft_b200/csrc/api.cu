@@ -36,6 +36,8 @@ struct gofft_plan {
   void *d_in = nullptr, *d_out = nullptr;
   size_t d_in_bytes = 0, d_out_bytes = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;  // host-pointer pipeline (2-D real plans)
+  std::vector<cudaEvent_t> host_ev;                     // per block: inputs on the device, block transformed
   std::mutex mu;
   int device = 0;
   bool cached = false;
@@ -43,6 +45,9 @@ struct gofft_plan {
     if (ws) cudaFree(ws);
     if (d_in) cudaFree(d_in);
     if (d_out) cudaFree(d_out);
+    for (cudaEvent_t e : host_ev) cudaEventDestroy(e);
+    if (copy_in) cudaStreamDestroy(copy_in);
+    if (copy_out) cudaStreamDestroy(copy_out);
     if (stream) cudaStreamDestroy(stream);
     if (lane) cudaStreamDestroy(lane);
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -363,6 +368,35 @@ static int exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, cudaS
 }
 
 
+// One block of nb images of a rank-2 real forward, on stream s with the
+// lane's pass workspace wsx.
+static int r2c_block(gofft_plan *p, const char *src, char *dst, long long nb, char *wsx, cudaStream_t s,
+                     double wsc) {
+  const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
+  // rows: real transform along the last axis (rfft2.go:41-51)
+  if (int e = p->rx->r2c(contig((void *)src, cols), contig(dst, rc), nb * rows, wsx, s, wsc)) return e;
+  // columns: complex transform down each of the rc columns (rfft2.go:53-72)
+  if (rows > 1) {
+    const Side cs = mk_side(dst, rows * rc, 1, rc, rc);
+    if (int e = p->ax[0]->exec(cs, cs, nb * rc, 0, 0, 1.0, wsx, s)) return e;
+  }
+  return GOFFT_OK;
+}
+
+// One block of nb images of a rank-2 real inverse: columns into the lane's
+// block buffer colbuf, then the real rows into dst.
+static int c2r_block(gofft_plan *p, const char *src, char *dst, long long nb, char *colbuf, char *wsx,
+                     cudaStream_t s, bool adj) {
+  const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
+  // columns: complex inverse, normalised by 1/rows (rfft2.go:100-120)
+  const Side cin = mk_side((void *)src, rows * rc, 1, rc, rc);
+  const Side cout = mk_side(colbuf, rows * rc, 1, rc, rc);
+  if (int e = p->ax[0]->exec(cin, cout, nb * rc, 1, 1, adj ? 1.0 : 1.0 / (double)rows, wsx, s)) return e;
+  // rows: real inverse of length cols (rfft2.go:122-136)
+  return p->rx->c2r(contig(colbuf, rc), (int)rc, contig(dst, cols), nb * rows, adj ? (double)cols : 1.0, wsx, s,
+                    adj);
+}
+
 // wsc != 0: the adjoint of the inverse (edge-bin weighting with scale wsc on
 // the row pass, the only real one).
 static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st, double wsc = 0.0) {
@@ -379,15 +413,7 @@ static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st, d
     const long long nb = std::min(p->chunk, p->batch - b0);
     const char *src = (const char *)in + (size_t)b0 * rows * cols * r;
     char *dst = (char *)out + (size_t)b0 * rows * rc * c;
-    const cudaStream_t s = ln.stream(blk);
-    char *wsx = ln.sub(blk);
-    // rows: real transform along the last axis (rfft2.go:41-51)
-    if (int e = p->rx->r2c(contig((void *)src, cols), contig(dst, rc), nb * rows, wsx, s, wsc)) return ln.join(e);
-    // columns: complex transform down each of the rc columns (rfft2.go:53-72)
-    if (rows > 1) {
-      const Side cs = mk_side(dst, rows * rc, 1, rc, rc);
-      if (int e = p->ax[0]->exec(cs, cs, nb * rc, 0, 0, 1.0, wsx, s)) return ln.join(e);
-    }
+    if (int e = r2c_block(p, src, dst, nb, ln.sub(blk), ln.stream(blk), wsc)) return ln.join(e);
   }
   return ln.join(GOFFT_OK);
 }
@@ -413,18 +439,7 @@ static int exec_c2r(gofft_plan *p, const void *in, long long nbins, void *out, c
     const long long nb = std::min(p->chunk, p->batch - b0);
     const char *src = (const char *)in + (size_t)b0 * rows * rc * c;
     char *dst = (char *)out + (size_t)b0 * rows * cols * r;
-    const cudaStream_t s = ln.stream(blk);
-    char *colbuf = ln.buf(blk);
-    char *wsx = ln.sub(blk);
-    // columns: complex inverse, normalised by 1/rows (rfft2.go:100-120)
-    const Side cin = mk_side((void *)src, rows * rc, 1, rc, rc);
-    const Side cout = mk_side(colbuf, rows * rc, 1, rc, rc);
-    if (int e = p->ax[0]->exec(cin, cout, nb * rc, 1, 1, adj ? 1.0 : 1.0 / (double)rows, wsx, s))
-      return ln.join(e);
-    // rows: real inverse of length cols (rfft2.go:122-136)
-    if (int e = p->rx->c2r(contig(colbuf, rc), (int)rc, contig(dst, cols), nb * rows, adj ? (double)cols : 1.0,
-                           wsx, s, adj))
-      return ln.join(e);
+    if (int e = c2r_block(p, src, dst, nb, ln.buf(blk), ln.sub(blk), ln.stream(blk), adj)) return ln.join(e);
   }
   return ln.join(GOFFT_OK);
 }
@@ -499,6 +514,76 @@ static int host_run(gofft_plan *p, const void *in, size_t in_b, void *out, size_
   return GOFFT_OK;
 }
 
+// Host-pointer execution of a rank-2 real plan, pipelined per block of
+// images: the host-to-device copy of block k+1 (copy-in stream), the
+// transforms of block k (on the block's lane) and the device-to-host copy of
+// block k-1 (copy-out stream) run at once, so both PCIe directions and the
+// GPU work together.  Blocks are half an L2 block (at least one image), which
+// keeps the pipeline's fill and drain short.  which: 1 forward, 2 inverse.
+static bool host_ranges_overlap(const void *a, size_t na, const void *b, size_t nb) {
+  const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+  return x < y + nb && y < x + na;
+}
+
+static int host_run_real2(gofft_plan *p, const void *in, void *out, int which) {
+  const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
+  const size_t rimg = (size_t)rows * cols * rsize(p->prec), cimg = (size_t)rows * rc * csize(p->prec);
+  const size_t in_img = which == 1 ? rimg : cimg, out_img = which == 1 ? cimg : rimg;
+  const long long hb = std::max<long long>(1, p->chunk / 2);
+  const long long nblk = (p->batch + hb - 1) / hb;
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (int e = ensure_staging(p, in_img * p->batch, out_img * p->batch)) return e;
+  if (!p->copy_in) GF_CK(cudaStreamCreateWithFlags(&p->copy_in, cudaStreamNonBlocking));
+  if (!p->copy_out) GF_CK(cudaStreamCreateWithFlags(&p->copy_out, cudaStreamNonBlocking));
+  while ((long long)p->host_ev.size() < 2 * nblk) {
+    cudaEvent_t e;
+    GF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    p->host_ev.push_back(e);
+  }
+  const bool two = p->nlanes > 1;
+  int rc_ = GOFFT_OK;
+  long long blk = 0;
+  for (long long b0 = 0; b0 < p->batch && rc_ == GOFFT_OK; b0 += hb, blk++) {
+    const long long nb = std::min(hb, p->batch - b0);
+    char *din = (char *)p->d_in + (size_t)b0 * in_img, *dout = (char *)p->d_out + (size_t)b0 * out_img;
+    cudaEvent_t ready = p->host_ev[2 * blk], done = p->host_ev[2 * blk + 1];
+    const cudaStream_t s = (two && (blk & 1)) ? p->lane : p->stream;
+    char *buf = (char *)p->ws + ((two && (blk & 1)) ? p->lane_bytes : 0);
+    cudaError_t ce = cudaMemcpyAsync(din, (const char *)in + (size_t)b0 * in_img, (size_t)nb * in_img,
+                                     cudaMemcpyHostToDevice, p->copy_in);
+    if (ce == cudaSuccess) ce = cudaEventRecord(ready, p->copy_in);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s, ready, 0);
+    if (ce != cudaSuccess) {
+      rc_ = set_err(GOFFT_ECUDA, std::string("host pipeline: ") + cudaGetErrorString(ce));
+      break;
+    }
+    rc_ = which == 1 ? r2c_block(p, din, dout, nb, buf + p->lane_buf, s, 0.0)
+                     : c2r_block(p, din, dout, nb, buf, buf + p->lane_buf, s, false);
+    if (rc_) break;
+    ce = cudaEventRecord(done, s);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(p->copy_out, done, 0);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync((char *)out + (size_t)b0 * out_img, dout, (size_t)nb * out_img, cudaMemcpyDeviceToHost,
+                           p->copy_out);
+    if (ce != cudaSuccess) rc_ = set_err(GOFFT_ECUDA, std::string("host pipeline: ") + cudaGetErrorString(ce));
+  }
+  // every stream drains before returning, on success and on error alike
+  cudaError_t e1 = cudaStreamSynchronize(p->copy_in);
+  cudaError_t e2 = cudaStreamSynchronize(p->stream);
+  cudaError_t e3 = two ? cudaStreamSynchronize(p->lane) : cudaSuccess;
+  cudaError_t e4 = cudaStreamSynchronize(p->copy_out);
+  if (rc_) return rc_;
+  for (cudaError_t e : {e1, e2, e3, e4})
+    if (e != cudaSuccess) return set_err(GOFFT_ECUDA, std::string("host pipeline: ") + cudaGetErrorString(e));
+  return GOFFT_OK;
+}
+
+// The pipelined path applies to batched 2-D real plans whose host buffers do
+// not overlap (an aliased output would overwrite inputs not yet copied).
+static bool use_real2_pipeline(const gofft_plan *p, const void *in, size_t in_b, const void *out, size_t out_b) {
+  return p->rank == 2 && p->batch > 1 && !host_ranges_overlap(in, in_b, out, out_b);
+}
+
 extern "C" int gofft_exec_c2c_host(gofft_plan *p, const void *in, void *out, int inverse) {
   if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
   if (p->kind != GOFFT_C2C) return set_err(GOFFT_EINVAL, "plan is not complex-to-complex");
@@ -507,11 +592,13 @@ extern "C" int gofft_exec_c2c_host(gofft_plan *p, const void *in, void *out, int
 extern "C" int gofft_exec_r2c_host(gofft_plan *p, const void *in, void *out) {
   if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
   if (p->kind != GOFFT_R2C) return set_err(GOFFT_EINVAL, "plan is not real");
+  if (use_real2_pipeline(p, in, real_bytes(p), out, bins_bytes(p))) return host_run_real2(p, in, out, 1);
   return host_run(p, in, real_bytes(p), out, bins_bytes(p), 1, 0, 0);
 }
 extern "C" int gofft_exec_c2r_host(gofft_plan *p, const void *in, int64_t nbins, void *out) {
   if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
   if (p->kind != GOFFT_R2C) return set_err(GOFFT_EINVAL, "plan is not real");
+  if (use_real2_pipeline(p, in, bins_bytes(p), out, real_bytes(p))) return host_run_real2(p, in, out, 2);
   return host_run(p, in, bins_bytes(p), out, real_bytes(p), 2, 0, nbins);
 }
 

@@ -114,6 +114,31 @@ def test_batched_rfft2_config2_shape():
     assert np.max(np.abs(back - x)) < 1e-12
 
 
+@pytest.mark.parametrize("pinned", [True, False])
+def test_batched_rfft2_host_pipeline(pinned):
+    # host-buffer RFFT2/IRFFT2 of a batch spanning several blocks on both
+    # lanes (copies, transforms and copies back overlapped per block) must
+    # give the device-buffer results
+    from fft_b200.device import DevicePlan
+    B = 8
+    x = rng(9).standard_normal((B, 1024 * 1024))
+    p = DevicePlan("r2c", "f64", [1024, 1024], batch=B)
+    dev = p.r2c(torch.from_numpy(x).cuda())
+    dev_back = p.c2r(dev).cpu().numpy()
+    dev = dev.cpu().numpy()
+    hx = torch.from_numpy(x)
+    hs = torch.zeros((B, 1024 * 513), dtype=torch.complex128)
+    hb = torch.zeros((B, 1024 * 1024), dtype=torch.float64)
+    if pinned:
+        hx, hs, hb = hx.pin_memory(), hs.pin_memory(), hb.pin_memory()
+    for _ in range(2):
+        p.r2c_host(hx.data_ptr(), hs.data_ptr())
+        assert rel_l2(hs.numpy(), dev) <= 1e-15
+        p.c2r_host(hs.data_ptr(), hb.data_ptr())
+        assert rel_l2(hb.numpy(), dev_back) <= 1e-15
+    assert rel_l2(hs.numpy()[B - 1], O.rfft2(x[B - 1].reshape(1024, 1024), 1024, 1024)) <= F64_TOL
+
+
 @pytest.mark.parametrize("prec", ["f32", "f32mixed"])
 def test_rfft2_fp32_forms(prec):
     from fft_b200.device import DevicePlan
