@@ -518,8 +518,12 @@ static int host_run(gofft_plan *p, const void *in, size_t in_b, void *out, size_
 // images: the host-to-device copy of block k+1 (copy-in stream), the
 // transforms of block k (on the block's lane) and the device-to-host copy of
 // block k-1 (copy-out stream) run at once, so both PCIe directions and the
-// GPU work together.  Blocks are half an L2 block (at least one image), which
-// keeps the pipeline's fill and drain short.  which: 1 forward, 2 inverse.
+// GPU work together.  Blocks are half an L2 block and never fewer than two
+// images (the configuration measured and tested; one-image blocks are not
+// used), which keeps the pipeline's fill and drain short.  which: 1 forward,
+// 2 inverse.
+static long long host_block_images(const gofft_plan *p) { return std::max<long long>(2, p->chunk / 2); }
+
 static bool host_ranges_overlap(const void *a, size_t na, const void *b, size_t nb) {
   const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
   return x < y + nb && y < x + na;
@@ -529,7 +533,7 @@ static int host_run_real2(gofft_plan *p, const void *in, void *out, int which) {
   const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
   const size_t rimg = (size_t)rows * cols * rsize(p->prec), cimg = (size_t)rows * rc * csize(p->prec);
   const size_t in_img = which == 1 ? rimg : cimg, out_img = which == 1 ? cimg : rimg;
-  const long long hb = std::max<long long>(1, p->chunk / 2);
+  const long long hb = host_block_images(p);
   const long long nblk = (p->batch + hb - 1) / hb;
   std::lock_guard<std::mutex> lk(p->mu);
   if (int e = ensure_staging(p, in_img * p->batch, out_img * p->batch)) return e;
@@ -578,10 +582,11 @@ static int host_run_real2(gofft_plan *p, const void *in, void *out, int which) {
   return GOFFT_OK;
 }
 
-// The pipelined path applies to batched 2-D real plans whose host buffers do
-// not overlap (an aliased output would overwrite inputs not yet copied).
+// The pipelined path applies to 2-D real plans with at least two blocks of
+// images and host buffers that do not overlap (an aliased output would
+// overwrite inputs not yet copied).
 static bool use_real2_pipeline(const gofft_plan *p, const void *in, size_t in_b, const void *out, size_t out_b) {
-  return p->rank == 2 && p->batch > 1 && !host_ranges_overlap(in, in_b, out, out_b);
+  return p->rank == 2 && p->batch >= 2 * host_block_images(p) && !host_ranges_overlap(in, in_b, out, out_b);
 }
 
 extern "C" int gofft_exec_c2c_host(gofft_plan *p, const void *in, void *out, int inverse) {
