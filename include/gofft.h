@@ -179,7 +179,10 @@ GOFFT_API int gofft_exec_c2c_noalloc(gofft_plan *p, const void *in, void *out, i
                                      gofft_stream stream);
 
 /* Host-pointer variants: copy host -> device, execute, copy back, synchronise.
- * Pinned host memory makes the copies asynchronous DMA. */
+ * Pinned host memory makes the copies asynchronous DMA.  Batched 2-D real
+ * plans (r2c / c2r) pipeline the batch in blocks of images: one block copies
+ * in while the previous one transforms and the one before copies out, so both
+ * PCIe directions overlap (rfft2.go:22-138 is the per-call reference path). */
 GOFFT_API int gofft_exec_c2c_host(gofft_plan *p, const void *in, void *out, int inverse);
 GOFFT_API int gofft_exec_r2c_host(gofft_plan *p, const void *in, void *out);
 GOFFT_API int gofft_exec_c2r_host(gofft_plan *p, const void *in, int64_t nbins, void *out);
