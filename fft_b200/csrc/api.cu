@@ -25,12 +25,12 @@ struct gofft_plan {
   std::vector<std::shared_ptr<const Exec1D>> ax;  // complex exec per axis
   std::shared_ptr<const ExecReal> rx;             // real exec of the last axis (R2C)
   long long chunk = 1;                            // images per L2 block (rank-2 R2C)
-  int nlanes = 1;                                 // streams the blocks alternate on
+  int nlanes = 1;                                 // streams the blocks rotate over (GOFFT_LANES, at most 3)
   size_t lane_bytes = 0;                          // workspace per lane
   size_t lane_buf = 0;                            // block buffer at the start of a lane region
   long long nplane_blocks = 0;                    // complex N-D: planes per L2 block (0: unblocked)
-  cudaStream_t lane = nullptr;                    // the second lane's stream
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t lane[2] = {nullptr, nullptr};      // the second and third lanes' streams
+  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
   size_t ws_bytes = 0;
   void *ws = nullptr;
   void *d_in = nullptr, *d_out = nullptr;
@@ -49,9 +49,11 @@ struct gofft_plan {
     if (copy_in) cudaStreamDestroy(copy_in);
     if (copy_out) cudaStreamDestroy(copy_out);
     if (stream) cudaStreamDestroy(stream);
-    if (lane) cudaStreamDestroy(lane);
+    for (int i = 0; i < 2; i++) {
+      if (lane[i]) cudaStreamDestroy(lane[i]);
+      if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+    }
     if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
   }
 };
 
@@ -71,17 +73,22 @@ static long long env_ll(const char *name, long long dflt) {
 
 // Items per L2 block for `units` items in at least `want` blocks: the
 // smallest block count from `want` up whose equal-as-possible blocks come out
-// even (when there are items for it), so the two lanes get the same number of
-// blocks instead of one lane running the last block alone.
-static long long lane_chunk(long long units, long long want) {
+// a multiple of the lane count (when there are items for it), so every lane
+// gets the same number of blocks instead of one lane running the last block
+// alone.
+static long long lane_chunk(long long units, long long want, int nl) {
   const long long first = (units + want - 1) / want;
   if (want <= 1) return first;
   for (long long nb = want; nb <= units; nb++) {
     const long long chunk = (units + nb - 1) / nb;
-    if (((units + chunk - 1) / chunk) % 2 == 0) return chunk;
+    if (((units + chunk - 1) / chunk) % nl == 0) return chunk;
   }
   return first;
 }
+
+// Lanes a blocked plan rotates its L2 blocks over: GOFFT_LANES (default 2),
+// between 1 and 3.
+static int lanes_wanted() { return (int)std::min<long long>(3, std::max<long long>(1, env_ll("GOFFT_LANES", 2))); }
 
 // Extent (elements) of `batch` lines of `len` elements at (dist, stride).
 static long long extent(long long batch, long long dist, long long len, long long stride) {
@@ -97,14 +104,14 @@ static int plan_ws(gofft_plan *p) {
       need = std::max(need, p->ax[a]->ws_bytes(lines));
     }
     if (p->nplane_blocks > 0) {
-      // two lane regions for the blocked last-two-axes passes
+      // one region per lane for the blocked last-two-axes passes
       const int r = p->rank;
       const long long kb = p->nplane_blocks;
       const size_t sub = std::max(p->ax[r - 1]->ws_bytes(kb * p->shape[r - 2]),
                                   p->ax[r - 2]->ws_bytes(kb * p->shape[r - 1]));
       p->lane_buf = 0;
       p->lane_bytes = (sub + 255) & ~(size_t)255;
-      need = std::max(need, 2 * p->lane_bytes);
+      need = std::max(need, (size_t)p->nlanes * p->lane_bytes);
     }
   } else if (p->rank == 1) {
     need = p->rx->ws_bytes(p->batch);
@@ -172,9 +179,9 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       const long long cmax =
           std::max<long long>(1, std::min<long long>(units, budget / (plane * (long long)csize(precision))));
       const long long nblocks = (units + cmax - 1) / cmax;
-      if (nblocks > 1 && env_ll("GOFFT_LANES", 2) >= 2) {
-        p->nplane_blocks = lane_chunk(units, nblocks);
-        p->nlanes = 2;
+      if (nblocks > 1 && lanes_wanted() >= 2) {
+        p->nlanes = lanes_wanted();
+        p->nplane_blocks = lane_chunk(units, nblocks, p->nlanes);
       }
     }
   } else {
@@ -191,19 +198,21 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       const long long per = p->shape[0] * rc * (long long)csize(precision);
       const long long cmax = std::max<long long>(1, std::min<long long>(batch, budget / std::max<long long>(1, per)));
       const long long nblocks = (batch + cmax - 1) / cmax;
-      // two lanes: block i+1's passes overlap block i's (each pass alone
-      // ramps up and drains; the other lane fills those gaps)
-      const bool lanes = nblocks > 1 && env_ll("GOFFT_LANES", 2) >= 2;
-      p->chunk = lanes ? lane_chunk(batch, nblocks) : (batch + nblocks - 1) / nblocks;  // balanced blocks
-      if (lanes) p->nlanes = 2;
+      // lanes: block i+1's passes overlap block i's (each pass alone ramps
+      // up and drains; the other lanes fill those gaps)
+      const bool lanes = nblocks > 1 && lanes_wanted() >= 2;
+      if (lanes) p->nlanes = lanes_wanted();
+      p->chunk = lanes ? lane_chunk(batch, nblocks, p->nlanes) : (batch + nblocks - 1) / nblocks;  // balanced blocks
     }
   }
   if (int rc2 = plan_ws(p.get())) return rc2;
   GF_CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   if (p->nlanes > 1) {
-    GF_CK(cudaStreamCreateWithFlags(&p->lane, cudaStreamNonBlocking));
     GF_CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
-    GF_CK(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
+    for (int i = 0; i + 1 < p->nlanes; i++) {
+      GF_CK(cudaStreamCreateWithFlags(&p->lane[i], cudaStreamNonBlocking));
+      GF_CK(cudaEventCreateWithFlags(&p->ev_join[i], cudaEventDisableTiming));
+    }
   }
   *out = p.release();
   return GOFFT_OK;
@@ -272,34 +281,41 @@ extern "C" int64_t gofft_plan_table(const gofft_plan *p, int which, int64_t *out
 // Execution on device pointers
 // ---------------------------------------------------------------------------
 // The L2 blocks of a plan (images of a rank-2 real plan, planes of a complex
-// N-D plan) alternate between the caller's stream and the plan's lane stream
+// N-D plan) rotate over the caller's stream and the plan's lane streams
 // (forked from and joined back into the caller's stream), each lane with its
 // own workspace region: the block buffer (real plans), then the passes'
 // workspace.
 struct Lanes {
   gofft_plan *p;
   cudaStream_t st;
-  bool two = false;
+  int n = 1;  // lanes in use
   Lanes(gofft_plan *p_, cudaStream_t st_) : p(p_), st(st_) {}
   int fork(long long nblocks) {
-    two = p->nlanes > 1 && nblocks > 1;
-    if (!two) return 0;
+    n = nblocks > 1 ? (int)std::min<long long>(p->nlanes, nblocks) : 1;
+    if (n == 1) return 0;
     GF_CK(cudaEventRecord(p->ev_fork, st));
-    GF_CK(cudaStreamWaitEvent(p->lane, p->ev_fork, 0));
+    for (int i = 0; i + 1 < n; i++) GF_CK(cudaStreamWaitEvent(p->lane[i], p->ev_fork, 0));
     return 0;
   }
-  cudaStream_t stream(long long blk) const { return (two && (blk & 1)) ? p->lane : st; }
-  char *buf(long long blk) const { return (char *)p->ws + ((two && (blk & 1)) ? p->lane_bytes : 0); }
+  int lane_of(long long blk) const { return n > 1 ? (int)(blk % n) : 0; }
+  cudaStream_t stream(long long blk) const {
+    const int k = lane_of(blk);
+    return k ? p->lane[k - 1] : st;
+  }
+  char *buf(long long blk) const { return (char *)p->ws + (size_t)lane_of(blk) * p->lane_bytes; }
   char *sub(long long blk) const { return buf(blk) + p->lane_buf; }
-  // Joins the lane back into the caller's stream; keeps the first error.
+  // Joins the lanes back into the caller's stream; keeps the first error.
   int join(int rc) {
-    if (!two) return rc;
-    two = false;
-    cudaError_t e1 = cudaEventRecord(p->ev_join, p->lane);
-    cudaError_t e2 = cudaStreamWaitEvent(st, p->ev_join, 0);
+    if (n == 1) return rc;
+    cudaError_t err = cudaSuccess;
+    for (int i = 0; i + 1 < n; i++) {
+      cudaError_t e1 = cudaEventRecord(p->ev_join[i], p->lane[i]);
+      cudaError_t e2 = cudaStreamWaitEvent(st, p->ev_join[i], 0);
+      if (err == cudaSuccess) err = e1 != cudaSuccess ? e1 : e2;
+    }
+    n = 1;
     if (rc) return rc;
-    if (e1 != cudaSuccess || e2 != cudaSuccess)
-      return set_err(GOFFT_ECUDA, std::string("lane join: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    if (err != cudaSuccess) return set_err(GOFFT_ECUDA, std::string("lane join: ") + cudaGetErrorString(err));
     return 0;
   }
 };
@@ -544,15 +560,16 @@ static int host_run_real2(gofft_plan *p, const void *in, void *out, int which) {
     GF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     p->host_ev.push_back(e);
   }
-  const bool two = p->nlanes > 1;
+  const int nl = std::max(1, p->nlanes);
   int rc_ = GOFFT_OK;
   long long blk = 0;
   for (long long b0 = 0; b0 < p->batch && rc_ == GOFFT_OK; b0 += hb, blk++) {
     const long long nb = std::min(hb, p->batch - b0);
     char *din = (char *)p->d_in + (size_t)b0 * in_img, *dout = (char *)p->d_out + (size_t)b0 * out_img;
     cudaEvent_t ready = p->host_ev[2 * blk], done = p->host_ev[2 * blk + 1];
-    const cudaStream_t s = (two && (blk & 1)) ? p->lane : p->stream;
-    char *buf = (char *)p->ws + ((two && (blk & 1)) ? p->lane_bytes : 0);
+    const int k = (int)(blk % nl);
+    const cudaStream_t s = k ? p->lane[k - 1] : p->stream;
+    char *buf = (char *)p->ws + (size_t)k * p->lane_bytes;
     cudaError_t ce = cudaMemcpyAsync(din, (const char *)in + (size_t)b0 * in_img, (size_t)nb * in_img,
                                      cudaMemcpyHostToDevice, p->copy_in);
     if (ce == cudaSuccess) ce = cudaEventRecord(ready, p->copy_in);
@@ -574,10 +591,11 @@ static int host_run_real2(gofft_plan *p, const void *in, void *out, int which) {
   // every stream drains before returning, on success and on error alike
   cudaError_t e1 = cudaStreamSynchronize(p->copy_in);
   cudaError_t e2 = cudaStreamSynchronize(p->stream);
-  cudaError_t e3 = two ? cudaStreamSynchronize(p->lane) : cudaSuccess;
+  cudaError_t e3 = nl > 1 ? cudaStreamSynchronize(p->lane[0]) : cudaSuccess;
+  cudaError_t e5 = nl > 2 ? cudaStreamSynchronize(p->lane[1]) : cudaSuccess;
   cudaError_t e4 = cudaStreamSynchronize(p->copy_out);
   if (rc_) return rc_;
-  for (cudaError_t e : {e1, e2, e3, e4})
+  for (cudaError_t e : {e1, e2, e3, e5, e4})
     if (e != cudaSuccess) return set_err(GOFFT_ECUDA, std::string("host pipeline: ") + cudaGetErrorString(e));
   return GOFFT_OK;
 }
