@@ -22,6 +22,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -83,14 +84,16 @@ class Clocks:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device):
+    def __init__(self, device, path=None):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench.csv")
+        if path is None:
+            fd, path = tempfile.mkstemp(prefix="gofft_clocks_", suffix=".csv")
+            os.close(fd)
+        self.path = path
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
@@ -165,6 +168,24 @@ def barrier(world):
 # ---------------------------------------------------------------------------
 # CPU arms (the oracle: C restatement of go-fft, all host threads)
 # ---------------------------------------------------------------------------
+def bench_config(batch, world):
+    """The workload description both arms report (identical dicts)."""
+    return {"workload": WORKLOAD, "images_per_step_per_gpu": batch, "rows": ROWS, "cols": COLS,
+            "l2": "inputs larger than L2 (%.0f MB per direction per GPU)" % (batch * ROWS * COLS * 8 / 1e6),
+            "parallelism": "replicas" if world == 1 else "batch-sharded x%d" % world}
+
+
+def cpu_model():
+    """The host CPU's model name (first 'model name' of /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for l in f:
+                if l.startswith("model name"):
+                    return l.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
 def cpu_time_images(n_images, seed=1):
     from oracle import oracle as O
     x = gen_images(n_images, seed)
@@ -189,7 +210,7 @@ def cpu_baseline(budget_s=10.0):
         passes += 1
     n = passes * x.shape[0]
     gbs = n * algo_bytes(8) / t / 1e9
-    return {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+    return {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "cpu_model": cpu_model(), "kind": "port",
             "sample": "%d passes over 8 images of the 1024x1024 float64 RFFT2+IRFFT2 round trip (%.1f s)"
                       % (passes, t),
             "transforms_per_s": round(2 * n / t, 2)}
@@ -202,7 +223,7 @@ def run_reference(args):
     from oracle import oracle as O
     O.set_workers(0)
     cores = O.get_workers()
-    per_step = 2
+    per_step = args.batch  # the GPU arm's images per step (same workload)
     x = gen_images(per_step, 1)
     for _ in range(args.warmup):
         O.batch_rfft2_roundtrip(x)
@@ -215,8 +236,9 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": round(1e3 * t / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOAD, "images_per_step": per_step, "rows": ROWS, "cols": COLS},
-            "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+            "config": bench_config(per_step, world),
+            "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "cpu_model": cpu_model(),
+                             "kind": "port",
                              "sample": "%d images per step x %d steps (C restatement of go-fft; no Go "
                                        "toolchain on this machine)" % (per_step, args.steps)},
             "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -227,25 +249,78 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def time_pipeline(plan, x, spec, back, steps, warmup, world, flush=None):
+REPEATS = 5  # timed repetitions of the K-step loop; the median is reported
+
+
+def time_pipeline(plan, x, spec, back, steps, warmup, world, repeats=REPEATS):
+    """Device time (s) of `steps` RFFT2+IRFFT2 steps, for each of `repeats`
+    repetitions of the step loop (CUDA events on the launching stream, a
+    barrier and a synchronize on both sides of each repetition)."""
     import torch
     for _ in range(warmup):
         plan.r2c(x, out=spec)
         plan.c2r(spec, out=back)
+    times = []
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        s = torch.cuda.current_stream()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(steps):
+            plan.r2c(x, out=spec)
+            plan.c2r(spec, out=back)
+        e1.record(s)
+        torch.cuda.synchronize()
+        barrier(world)
+        times.append(e0.elapsed_time(e1) / 1e3)
+    return times
+
+
+def plan_costs():
+    """Plan construction time on the GPU beside go-fft's NewPlan
+    (BENCHMARKS.md:125-141: 1024 -> 14.8 us, 10007 -> 993 us on an M4 Max).
+    `cold` is the first plan of a length in this process: it generates the
+    device tables (twiddles, Rader permutations and kernel spectrum) and
+    compiles nothing.  `warm` is the median of later plans of the same length,
+    which reuse the per-length device programs the way go-fft's cachedPlan
+    reuses its sub-plans, and only set up the plan object (streams,
+    workspace).  Host wall clock around the synchronous C-ABI call."""
+    import torch
+    from fft_b200._lib import GOFFT_C2C, GOFFT_F64, GOFFT_R2C, check, lib
+    torch.zeros(1, device="cuda")  # the CUDA context exists before timing
     torch.cuda.synchronize()
-    barrier(world)
-    torch.cuda.synchronize()
-    s = torch.cuda.current_stream()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(s)
-    for _ in range(steps):
-        plan.r2c(x, out=spec)
-        plan.c2r(spec, out=back)
-    e1.record(s)
-    torch.cuda.synchronize()
-    barrier(world)
-    return e0.elapsed_time(e1) / 1e3
+    out = {}
+
+    def create(kind, shape):
+        h = ctypes.c_void_p()
+        sh = (ctypes.c_int64 * len(shape))(*shape)
+        t0 = time.perf_counter()
+        check(lib().gofft_plan_create(kind, GOFFT_F64, sh, len(shape), 1, 0, 0, 0, 0, ctypes.byref(h)))
+        dt = time.perf_counter() - t0
+        lib().gofft_plan_destroy(h)
+        return dt
+
+    def new_plan(n):
+        h = ctypes.c_void_p()
+        t0 = time.perf_counter()
+        check(lib().gofft_new_plan(n, ctypes.byref(h)))
+        dt = time.perf_counter() - t0
+        lib().gofft_plan_destroy(h)
+        return dt
+
+    cases = [("NewPlan(1024)", lambda: new_plan(1024), 14.808),
+             ("NewPlan(10007)", lambda: new_plan(10007), 993.365),
+             ("c2c 65536", lambda: create(GOFFT_C2C, [65536]), None),
+             ("r2c 1024x1024", lambda: create(GOFFT_R2C, [1024, 1024]), None)]
+    for name, fn, ref_us in cases:
+        cold = fn()
+        warm = statistics.median(fn() for _ in range(20))
+        out[name] = {"cold_us": round(cold * 1e6, 1), "warm_us": round(warm * 1e6, 1),
+                     "reference_us_m4max": ref_us}
+    return out
 
 
 def _events_ms(torch, fn, reps, warm=3):
@@ -432,6 +507,8 @@ def run_ours(args):
     torch.cuda.set_device(local)
     B = args.batch
     peak, peak_kind = peaks()
+    # plan construction cost, first thing (cold = no length built yet)
+    pcost = plan_costs() if rank == 0 else None
 
     # the engine's own autotuner picks radix schedules and lines per CTA for
     # this shape (setup, before any timed work)
@@ -456,9 +533,10 @@ def run_ours(args):
 
     n0 = _lib.launch_count()
     with Clocks(local) as clk:
-        t64 = time_pipeline(p64, x64, s64, b64, args.steps, args.warmup, world)
-    launches = (_lib.launch_count() - n0) * args.steps // (args.steps + args.warmup)
-    t64 = max_over_ranks(t64, world)
+        reps64 = time_pipeline(p64, x64, s64, b64, args.steps, args.warmup, world)
+    launches = (_lib.launch_count() - n0) * args.steps // (args.warmup + REPEATS * args.steps)
+    reps64 = [max_over_ranks(t, world) for t in reps64]
+    t64 = statistics.median(reps64)
     gbs64 = world * args.steps * B * algo_bytes(8) / t64 / 1e9
 
     # FP32-mixed form on the same images (rounded to float32)
@@ -466,23 +544,40 @@ def run_ours(args):
     p32 = DevicePlan("r2c", "f32mixed", [ROWS, COLS], batch=B)
     s32 = torch.empty((B, ROWS * RC), dtype=torch.complex64, device="cuda")
     b32 = torch.empty_like(x32)
-    t32 = time_pipeline(p32, x32, s32, b32, args.steps, args.warmup, world)
-    t32 = max_over_ranks(t32, world)
+    reps32 = time_pipeline(p32, x32, s32, b32, args.steps, args.warmup, world)
+    reps32 = [max_over_ranks(t, world) for t in reps32]
+    t32 = statistics.median(reps32)
     gbs32 = world * args.steps * B * algo_bytes(4) / t32 / 1e9
 
-    # per-kernel timing of the FP64 step with CUDA events (separate pass)
-    _lib.timing_enable(True)
-    _lib.timing_report()
+    # per-kernel timing of the FP64 step with CUDA events on the launch stream
+    # (separate passes): a one-lane plan runs every launch alone, so each
+    # kernel's events time that kernel only; the two-lane plan's figures (the
+    # bench's own, with the next block's launches overlapping) are kept beside
+    from fft_b200 import tune as _tune
+
+    def kernel_times(plan, nrep):
+        _lib.timing_enable(True)
+        _lib.timing_report()
+        for _ in range(nrep):
+            plan.r2c(x64, out=s64)
+            plan.c2r(s64, out=b64)
+        torch.cuda.synchronize()
+        rep = _lib.timing_report()
+        _lib.timing_enable(False)
+        return rep
+
     nrep = max(3, min(args.steps, 20))
-    for _ in range(nrep):
-        p64.r2c(x64, out=s64)
-        p64.c2r(s64, out=b64)
-    torch.cuda.synchronize()
-    rep = _lib.timing_report()
-    _lib.timing_enable(False)
+    _tune.set_lanes(1)
+    p64_one = DevicePlan("r2c", "f64", [ROWS, COLS], batch=B)
+    _tune.set_lanes(0)
+    kernel_times(p64_one, 2)  # warm-up
+    rep = kernel_times(p64_one, nrep)
+    rep2 = kernel_times(p64, nrep)
+    p64_one.close()
     dom = max(rep, key=lambda r: r["ms"])
     total_ms = sum(r["ms"] for r in rep)
     achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9
+    dom2 = max(rep2, key=lambda r: r["ms"])
     # measured DRAM traffic of one launch of the dominant kernel
     key = "/".join(dom["kernel"].split("/")[:3])
     traffic = None
@@ -533,27 +628,34 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": round(gbs64, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * t64 / args.steps, 4), "higher_is_better": True,
+        "repeats": {"count": REPEATS, "statistic": "median",
+                    "ms_per_step": [round(1e3 * t / args.steps, 4) for t in reps64]},
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "images_per_step_per_gpu": B, "rows": ROWS, "cols": COLS,
-                   "l2": "inputs larger than L2 (%.0f MB per direction per GPU)" % (B * ROWS * COLS * 8 / 1e6),
-                   "parallelism": "replicas" if world == 1 else "batch-sharded x%d" % world,
-                   "autotuned": {"schedule": wisdom32["schedule"], "lpc": wisdom32["lpc"]}},
+        "config": bench_config(B, world),
+        "autotuned": {"schedule": wisdom32["schedule"], "lpc": wisdom32["lpc"]},
         "transforms_per_s": round(world * args.steps * B * 2 / t64, 1),
         "hbm_frac": round(gbs64 / world / peak, 4),
         "rel_l2_f64_vs_oracle": rel64, "roundtrip_max_abs_f64": rt64,
         "mixed": {"value": round(gbs32, 2), "unit": "GB/s", "dtype": "f32 (hi+lo twiddles)",
                   "transforms_per_s": round(world * args.steps * B * 2 / t32, 1),
                   "speedup_vs_f64": round(t64 / t32, 3), "rel_l2_vs_f64_oracle": rel32,
-                  "max_abs_vs_f64_oracle": maxabs32, "ms_per_step": round(1e3 * t32 / args.steps, 4)},
+                  "max_abs_vs_f64_oracle": maxabs32, "ms_per_step": round(1e3 * t32 / args.steps, 4),
+                  "repeats_ms_per_step": [round(1e3 * t / args.steps, 4) for t in reps32]},
         "roofline": {"bound": "hbm", "kernel": dom["kernel"], "achieved": round(achieved, 1),
                      "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": round(dom["bytes"] / dom["launches"]),
                      "share": round(dom["ms"] / total_ms, 3),
+                     "timed": "one lane (each launch alone), CUDA events on the launch stream",
                      "kernels": [{"kernel": r["kernel"], "launches": r["launches"],
                                   "avg_us": round(1e3 * r["ms"] / r["launches"], 2),
                                   "gbs": round(r["bytes"] / (r["ms"] / 1e3) / 1e9, 1),
-                                  "share": round(r["ms"] / total_ms, 3)} for r in rep]},
+                                  "share": round(r["ms"] / total_ms, 3)} for r in rep],
+                     "two_lanes": {"kernel": dom2["kernel"],
+                                   "achieved": round(dom2["bytes"] / (dom2["ms"] / 1e3) / 1e9, 1),
+                                   "note": "the bench plan's own launches; a kernel's events also span the "
+                                           "other lane's overlapping work"}},
+        "plan_construction": pcost,
         "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu,
         "other_workloads": extra,
     }

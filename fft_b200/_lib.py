@@ -82,6 +82,8 @@ SIGNATURES = {
     "gofft_timing_report": (_i64, [ctypes.c_char_p, _i64]),
     "gofft_set_lines_per_cta": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gofft_set_pipelined": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int, ctypes.c_int]),
+    "gofft_set_l2_block_bytes": (ctypes.c_int, [_i64]),
+    "gofft_set_lanes": (ctypes.c_int, [ctypes.c_int]),
     "gofft_set_schedule": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int]),
     "gofft_hamming": (ctypes.c_int, [_i64, _vp]),
     "gofft_blackman": (ctypes.c_int, [_i64, _vp]),

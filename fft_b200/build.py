@@ -4,7 +4,7 @@ Each CUDA translation unit under csrc/ is compiled in parallel with
 ``nvcc -gencode arch=compute_100a,code=sm_100a`` and linked into one shared
 library with the CUDA runtime linked statically, so the library loads without
 torch and only needs the NVIDIA driver.  Objects go to csrc/_build/ and are
-rebuilt when any source or header is newer.
+rebuilt when the source or a project header it includes is newer.
 
     python -m fft_b200.build [--force] [--verbose]
 """
@@ -12,6 +12,7 @@ import argparse
 import concurrent.futures
 import glob
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -34,17 +35,35 @@ def nvcc():
     return exe
 
 
-def _newest_header():
-    hs = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
-    hs += glob.glob(os.path.join(INCLUDE, "*.h"))
-    return max((os.path.getmtime(h) for h in hs), default=0)
+_INC = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _local_deps(path, seen=None):
+    """The project headers `path` includes, directly or through other
+    project headers (quoted includes resolved against the including file's
+    folder, csrc/ and include/)."""
+    seen = set() if seen is None else seen
+    try:
+        text = open(path).read()
+    except OSError:
+        return seen
+    for name in _INC.findall(text):
+        for base in (os.path.dirname(path), CSRC, INCLUDE):
+            h = os.path.normpath(os.path.join(base, name))
+            if os.path.exists(h):
+                if h not in seen:
+                    seen.add(h)
+                    _local_deps(h, seen)
+                break
+    return seen
 
 
 def _compile(src, force, verbose):
     obj = os.path.join(OBJ, os.path.basename(src).replace(".cu", ".o"))
     if not force and os.path.exists(obj):
         t = os.path.getmtime(obj)
-        if t >= os.path.getmtime(src) and t >= _newest_header():
+        newest = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in _local_deps(src)])
+        if t >= newest:
             return obj, ""
     cmd = [nvcc()] + ARCH + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)

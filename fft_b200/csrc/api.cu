@@ -1,6 +1,7 @@
 // api.cu -- the C-ABI (include/gofft.h): device-resident plans and the
 // reference-facing entry points that mirror go-fft/fft's Go API.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -25,11 +26,11 @@ struct gofft_plan {
   std::vector<std::shared_ptr<const Exec1D>> ax;  // complex exec per axis
   std::shared_ptr<const ExecReal> rx;             // real exec of the last axis (R2C)
   long long chunk = 1;                            // images per L2 block (rank-2 R2C)
-  int nlanes = 1;                                 // streams the blocks rotate over (GOFFT_LANES, at most 3)
+  int nlanes = 1;                                 // streams the blocks rotate over (1 or kLanes)
   size_t lane_bytes = 0;                          // workspace per lane
   size_t lane_buf = 0;                            // block buffer at the start of a lane region
   long long nplane_blocks = 0;                    // complex N-D: planes per L2 block (0: unblocked)
-  cudaStream_t lane[2] = {nullptr, nullptr};      // the second and third lanes' streams
+  cudaStream_t lane[2] = {nullptr, nullptr};      // the second lane's stream (lane[1] unused)
   cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
   size_t ws_bytes = 0;
   void *ws = nullptr;
@@ -65,11 +66,13 @@ extern "C" const char *gofft_version(void) { return kVersion; }
 // ---------------------------------------------------------------------------
 // Plan construction
 // ---------------------------------------------------------------------------
-static long long env_ll(const char *name, long long dflt) {
-  const char *v = getenv(name);
-  if (!v || !*v) return dflt;
-  return atoll(v);
-}
+// Bytes of complex intermediate an L2 block of images (rank-2 real plans) or
+// planes (complex N-D plans) may hold, so the row-to-column intermediate stays
+// in the 126 MB L2; process-wide, read when a plan is created
+// (gofft_set_l2_block_bytes).
+static constexpr long long kL2BlockBytes = 48ll << 20;
+static std::atomic<long long> g_l2_block_bytes{kL2BlockBytes};
+static long long l2_block_bytes() { return g_l2_block_bytes.load(); }
 
 // Items per L2 block for `units` items in at least `want` blocks: the
 // smallest block count from `want` up whose equal-as-possible blocks come out
@@ -86,9 +89,12 @@ static long long lane_chunk(long long units, long long want, int nl) {
   return first;
 }
 
-// Lanes a blocked plan rotates its L2 blocks over: GOFFT_LANES (default 2),
-// between 1 and 3.
-static int lanes_wanted() { return (int)std::min<long long>(3, std::max<long long>(1, env_ll("GOFFT_LANES", 2))); }
+// Lanes (streams) a blocked plan rotates its L2 blocks over, for plans created
+// afterwards (gofft_set_lanes): two by default, measured best on the 2-D real
+// round trip (three: 0.494-0.510 ms against 0.483 ms); one runs the blocks
+// back to back on the caller's stream, so each pass is timed alone.
+static constexpr int kLanes = 2;
+static std::atomic<int> g_lanes{kLanes};
 
 // Extent (elements) of `batch` lines of `len` elements at (dist, stride).
 static long long extent(long long batch, long long dist, long long len, long long stride) {
@@ -175,12 +181,12 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       const long long plane = p->shape[rank - 1] * p->shape[rank - 2];
       const bool merged = p->idist == p->total && p->odist == p->total;
       const long long units = (merged ? batch : 1) * (p->total / plane);
-      const long long budget = env_ll("GOFFT_L2_BLOCK_BYTES", 48ll << 20);
+      const long long budget = l2_block_bytes();
       const long long cmax =
           std::max<long long>(1, std::min<long long>(units, budget / (plane * (long long)csize(precision))));
       const long long nblocks = (units + cmax - 1) / cmax;
-      if (nblocks > 1 && lanes_wanted() >= 2) {
-        p->nlanes = lanes_wanted();
+      if (nblocks > 1 && g_lanes.load() > 1) {
+        p->nlanes = g_lanes.load();
         p->nplane_blocks = lane_chunk(units, nblocks, p->nlanes);
       }
     }
@@ -194,14 +200,14 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       if (p->istride != 1 || p->idist != p->total || p->ostride != 1 || p->odist != p->shape[0] * rc)
         return set_err(GOFFT_EUNSUPPORTED, "2-D real transforms need contiguous images");
       // images per block: keep a block's complex intermediate L2-resident
-      const long long budget = env_ll("GOFFT_L2_BLOCK_BYTES", 48ll << 20);
+      const long long budget = l2_block_bytes();
       const long long per = p->shape[0] * rc * (long long)csize(precision);
       const long long cmax = std::max<long long>(1, std::min<long long>(batch, budget / std::max<long long>(1, per)));
       const long long nblocks = (batch + cmax - 1) / cmax;
       // lanes: block i+1's passes overlap block i's (each pass alone ramps
       // up and drains; the other lanes fill those gaps)
-      const bool lanes = nblocks > 1 && lanes_wanted() >= 2;
-      if (lanes) p->nlanes = lanes_wanted();
+      const bool lanes = nblocks > 1 && g_lanes.load() > 1;
+      if (lanes) p->nlanes = g_lanes.load();
       p->chunk = lanes ? lane_chunk(batch, nblocks, p->nlanes) : (batch + nblocks - 1) / nblocks;  // balanced blocks
     }
   }
@@ -602,9 +608,13 @@ static int host_run_real2(gofft_plan *p, const void *in, void *out, int which) {
 
 // The pipelined path applies to 2-D real plans with at least two blocks of
 // images and host buffers that do not overlap (an aliased output would
-// overwrite inputs not yet copied).
+// overwrite inputs not yet copied).  A host block runs through one lane's
+// workspace, which holds `chunk` images (one L2 block): plans whose host
+// block would be larger (chunk < 2, i.e. one image's spectrum fills more than
+// half the L2 block budget) take the serial path instead.
 static bool use_real2_pipeline(const gofft_plan *p, const void *in, size_t in_b, const void *out, size_t out_b) {
-  return p->rank == 2 && p->batch >= 2 * host_block_images(p) && !host_ranges_overlap(in, in_b, out, out_b);
+  return p->rank == 2 && host_block_images(p) <= p->chunk && p->batch >= 2 * host_block_images(p) &&
+         !host_ranges_overlap(in, in_b, out, out_b);
 }
 
 extern "C" int gofft_exec_c2c_host(gofft_plan *p, const void *in, void *out, int inverse) {
@@ -1101,6 +1111,15 @@ extern "C" int gofft_set_lines_per_cta(int precision, int64_t n, int op, int col
   set_lpc_override(precision, n, op, colmode, lpc);
   return GOFFT_OK;
 }
+extern "C" int gofft_set_l2_block_bytes(int64_t bytes) {
+  g_l2_block_bytes.store(bytes > 0 ? bytes : kL2BlockBytes);
+  return GOFFT_OK;
+}
+extern "C" int gofft_set_lanes(int lanes) {
+  if (lanes < 0 || lanes > 2) return set_err(GOFFT_EINVAL, "lanes must be 1 or 2 (0: the default)");
+  g_lanes.store(lanes == 0 ? kLanes : lanes);
+  return GOFFT_OK;
+}
 extern "C" int gofft_set_pipelined(int precision, int64_t n, int op, int on) {
   set_pipe_override(precision, n, op, on);
   return GOFFT_OK;
@@ -1300,8 +1319,8 @@ static std::map<int, void *> g_noalloc_addr;
 extern "C" int gofft_exec_c2c_noalloc(gofft_plan *p, const void *in, void *out, int inverse,
                                       gofft_stream stream) {
   if (!p || !in || !out) return set_err(GOFFT_EINVAL, "null argument");
-  if (p->kind != GOFFT_C2C || p->rank != 1)
-    return set_err(GOFFT_EUNSUPPORTED, "the no-allocation entry point takes 1-D complex plans");
+  if (p->kind != GOFFT_C2C) return set_err(GOFFT_EINVAL, "plan is not complex-to-complex");
+  if (p->rank != 1) return set_err(GOFFT_EUNSUPPORTED, "the no-allocation entry point takes 1-D complex plans");
   const size_t need = p->ax[0]->ws_bytes(p->batch);
   if (need > kNoAllocScratchBytes)
     return set_err(GOFFT_EINVAL, "transform needs " + std::to_string(need) +

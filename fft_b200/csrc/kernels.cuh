@@ -64,8 +64,10 @@ __global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
 // of that phase is done: its items come later in the numbering, so the
 // prerequisite's items were claimed by running CTAs that never wait on later
 // items, and the wait ends.  Each wait is bounded: past spin_limit polls the
-// CTA sets *err and carries on (results are then invalid and the host reports
-// a timeout).
+// CTA sets *err (results are then invalid and the host reports a timeout).
+// Once *err is set, every CTA stops waiting and skips the remaining items'
+// transforms (still counting them done), so the kernel drains at once
+// instead of spending spin_limit polls on each later dependent item.
 // ---------------------------------------------------------------------------
 struct PhaseDesc {
   KArgs a;
@@ -144,11 +146,12 @@ __global__ void __launch_bounds__(512, 1) k_persist(const PhaseDesc *ph, int nph
   __shared__ __align__(16) unsigned char sa_raw[sizeof(KArgs)];
   KArgs &sa = *reinterpret_cast<KArgs *>(sa_raw);
   __shared__ long long s_item;
-  __shared__ int s_p;
+  __shared__ int s_p, s_failed;
   for (;;) {
     if (threadIdx.x == 0) {
       const long long it = (long long)atomicAdd(ctr, 1ull);
       s_item = it;
+      s_failed = *((volatile int *)err);
       if (it < total) {
         int lo = 0, hi = nph - 1;
         while (lo < hi) {
@@ -158,12 +161,17 @@ __global__ void __launch_bounds__(512, 1) k_persist(const PhaseDesc *ph, int nph
         }
         s_p = lo;
         const int d = ph[lo].dep;
-        if (d >= 0) {
+        if (d >= 0 && !s_failed) {
           const int need = (int)ph[d].ntiles;
           long long polls = 0;
           while (*((volatile int *)&done[d]) < need) {
+            if (*((volatile int *)err)) {  // another CTA gave up: drain
+              s_failed = 1;
+              break;
+            }
             if (++polls > spin_limit) {
               atomicExch(err, 1);
+              s_failed = 1;
               break;
             }
             __nanosleep(128);
@@ -176,15 +184,17 @@ __global__ void __launch_bounds__(512, 1) k_persist(const PhaseDesc *ph, int nph
     const long long item = s_item;
     if (item >= total) break;
     const int p = s_p;
-    {
-      const int *src = reinterpret_cast<const int *>(&ph[p].a);
-      int *dst = reinterpret_cast<int *>(&sa);
-      for (int i = threadIdx.x; i < (int)(sizeof(KArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    if (!s_failed) {
+      {
+        const int *src = reinterpret_cast<const int *>(&ph[p].a);
+        int *dst = reinterpret_cast<int *>(&sa);
+        for (int i = threadIdx.x; i < (int)(sizeof(KArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+      }
+      __syncthreads();
+      const bool active = threadIdx.x < sa.lpc * sa.lp.T;
+      phase_dispatch<P>(sa, ph[p].op, item - ph[p].first, active);
+      __threadfence();
     }
-    __syncthreads();
-    const bool active = threadIdx.x < sa.lpc * sa.lp.T;
-    phase_dispatch<P>(sa, ph[p].op, item - ph[p].first, active);
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) atomicAdd(&done[p], 1);
   }

@@ -594,19 +594,14 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   // direct stages index a line with 32-bit element offsets
   if (std::max(std::llabs(a.in.stride), std::llabs(a.out.stride)) * (long long)dp.n >= (1ll << 31))
     a.flags &= GF_COLMAP;
-  if (const char *e = getenv("GOFFT_NO_DIRECT")) {
-    if (*e == '1') a.flags &= GF_COLMAP;
-  }
   size_t smem = (size_t)lpc * spad_size(dp.n) * csize(dp.prec) + (conv ? 2 * lpc * csize(dp.prec) : 0);
   KFn f = nullptr;
-  static const bool no_ct = getenv("GOFFT_NO_CT") && getenv("GOFFT_NO_CT")[0] == '1';
   // the persistent double-buffered variant halves resident CTAs; measured
-  // slower on the 1024/512-point lines, so it is opt-in (GOFFT_PIPE=1 or the
-  // autotuner's pipe choice)
-  static const bool env_pipe = getenv("GOFFT_PIPE") && getenv("GOFFT_PIPE")[0] == '1';
-  const bool no_pipe = !(env_pipe || get_pipe_override(dp.prec, dp.n, op));
+  // slower on the 1024/512-point lines, so it is opt-in (the autotuner's
+  // pipe choice, gofft_set_pipelined)
+  const bool no_pipe = !get_pipe_override(dp.prec, dp.n, op);
   long long grid = (nlines + lpc - 1) / lpc;
-  if (!no_ct) {
+  {
     // persistent double-buffered variant when two tile buffers fit
     if (!conv && !no_pipe && 2 * smem <= max_smem_optin() && grid > 2 * num_sms()) {
       f = kernel_ct_for(dp, op, lpc, true);

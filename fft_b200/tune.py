@@ -5,6 +5,7 @@ C-ABI).  No counterpart in go-fft/fft, whose plans are fixed by its router.
     text = export_wisdom()          # JSON, for a file
     import_wisdom(text)             # in a later process, before planning
     forget_wisdom()                 # back to the built-in defaults
+    set_l2_block_bytes(1 << 20)     # smaller L2 blocks for plans created next
 
 Settings are process-wide per (precision, length): plans created after a
 tune or an import use them; plans created before keep theirs.
@@ -56,3 +57,16 @@ def import_wisdom(text):
 
 def forget_wisdom():
     check(lib().gofft_wisdom_forget())
+
+
+def set_l2_block_bytes(nbytes):
+    """Complex intermediate bytes per L2 block for plans created afterwards
+    (rank-2 real plans: images per block; complex N-D plans: planes per
+    block); nbytes <= 0 restores the default of 48 MiB."""
+    check(lib().gofft_set_l2_block_bytes(int(nbytes)))
+
+
+def set_lanes(lanes):
+    """Streams plans created afterwards rotate their L2 blocks over: 2 (the
+    default; 0 restores it) or 1 (blocks back to back, each pass alone)."""
+    check(lib().gofft_set_lanes(int(lanes)))

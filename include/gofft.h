@@ -172,9 +172,11 @@ GOFFT_API int gofft_exec_c2r(gofft_plan *p, const void *in, int64_t nbins, void 
  * budget, or paths that cannot afford cudaMalloc's device-wide
  * synchronisation.  Scratch comes from one 16 MiB array built into the
  * library (held on every GPU that loads it); transforms needing more return
- * GOFFT_EINVAL.  The first call on a device looks the array up and should come
- * before any stream capture.  All calls share the array: calls whose
- * executions overlap on the GPU race and must be serialised by the caller. */
+ * GOFFT_EINVAL, a plan that is not complex-to-complex GOFFT_EINVAL, and a
+ * complex plan of rank above 1 GOFFT_EUNSUPPORTED.  The first call on a device
+ * looks the array up and should come before any stream capture.  All calls
+ * share the array: calls whose executions overlap on the GPU race and must be
+ * serialised by the caller. */
 GOFFT_API int gofft_exec_c2c_noalloc(gofft_plan *p, const void *in, void *out, int inverse,
                                      gofft_stream stream);
 
@@ -311,6 +313,17 @@ GOFFT_API int64_t gofft_timing_report(char *buf, int64_t cap);
 /* Overrides the lines-per-CTA of the line kernel for (precision, length n,
  * op, column mode); lpc <= 0 restores the heuristic.  Used by the autotuner. */
 GOFFT_API int gofft_set_lines_per_cta(int precision, int64_t n, int op, int colmode, int lpc);
+/* Bytes of complex intermediate one L2 block may hold in plans created
+ * afterwards: rank-2 real plans run their row and column passes per block of
+ * images, complex N-D plans their last two axes per block of planes, so the
+ * intermediate stays in L2.  bytes <= 0 restores the default (48 MiB).  A
+ * tuning knob (process-wide); results do not depend on it. */
+GOFFT_API int gofft_set_l2_block_bytes(int64_t bytes);
+/* Streams ("lanes") that plans created afterwards rotate their L2 blocks
+ * over: 2 (the default, 0 restores it) overlaps one block's passes with the
+ * next block's; 1 runs the blocks one after another on the caller's stream
+ * (each pass then runs alone, e.g. to time it).  GOFFT_EINVAL otherwise. */
+GOFFT_API int gofft_set_lanes(int lanes);
 /* Selects (on = 1) the persistent double-buffered line kernel for
  * (precision, n, op) where one exists.  Used by the autotuner. */
 GOFFT_API int gofft_set_pipelined(int precision, int64_t n, int op, int on);

@@ -139,6 +139,45 @@ def test_batched_rfft2_host_pipeline(pinned):
     assert rel_l2(hs.numpy()[B - 1], O.rfft2(x[B - 1].reshape(1024, 1024), 1024, 1024)) <= F64_TOL
 
 
+@pytest.fixture
+def small_l2_blocks():
+    """A 1 MiB L2 block budget for the plans a test creates (restored after)."""
+    from fft_b200 import tune
+    tune.set_l2_block_bytes(1 << 20)
+    yield 1 << 20
+    tune.set_l2_block_bytes(0)
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_pipeline_one_image_blocks(pinned, small_l2_blocks):
+    """A plan whose L2 block holds one image (each 256x256 float64 spectrum,
+    526 KB, is more than half the 1 MiB budget): the host-buffer calls must not
+    form blocks larger than a lane's workspace.  They take the serial path and
+    match the device-buffer results exactly and the oracle at 1e-12."""
+    from fft_b200.device import DevicePlan
+    B, R, C = 6, 256, 256
+    K = C // 2 + 1
+    p = DevicePlan("r2c", "f64", [R, C], batch=B)
+    assert p.describe()["chunk"] == 1
+    x = rng(21).standard_normal((B, R * C))
+    dev = p.r2c(torch.from_numpy(x).cuda())
+    dev_back = p.c2r(dev).cpu().numpy()
+    dev = dev.cpu().numpy()
+    hx = torch.from_numpy(x)
+    hs = torch.zeros((B, R * K), dtype=torch.complex128)
+    hb = torch.zeros((B, R * C), dtype=torch.float64)
+    if pinned:
+        hx, hs, hb = hx.pin_memory(), hs.pin_memory(), hb.pin_memory()
+    for _ in range(2):
+        p.r2c_host(hx.data_ptr(), hs.data_ptr())
+        assert np.array_equal(hs.numpy(), dev)
+        p.c2r_host(hs.data_ptr(), hb.data_ptr())
+        assert np.array_equal(hb.numpy(), dev_back)
+    for b in range(B):
+        assert rel_l2(hs.numpy()[b], O.rfft2(x[b].reshape(R, C), R, C)) <= F64_TOL
+        assert np.max(np.abs(hb.numpy()[b] - x[b])) < 1e-12
+
+
 @pytest.mark.parametrize("prec", ["f32", "f32mixed"])
 def test_rfft2_fp32_forms(prec):
     from fft_b200.device import DevicePlan
@@ -195,12 +234,11 @@ def test_device_spectrogram_fp32(prec):
 @pytest.mark.parametrize("prec", ["f64", "f32mixed"])
 @pytest.mark.parametrize("shape,batch,gap", [([40, 64, 96], 1, 0), ([64, 96], 40, 0), ([20, 32, 48], 2, 5),
                                             ([6, 5, 64, 1009], 1, 0), ([10, 360, 48], 3, 0)])
-def test_fftn_plane_blocks(prec, shape, batch, gap, monkeypatch):
+def test_fftn_plane_blocks(prec, shape, batch, gap, small_l2_blocks):
     """Complex N-D transforms whose last two axes run per L2 block of planes
     on two lanes (a small block budget forces several blocks), against the
     oracle: merged and gapped batches, prime and smooth axes."""
     from fft_b200.device import DevicePlan
-    monkeypatch.setenv("GOFFT_L2_BLOCK_BYTES", str(1 << 20))
     n = int(np.prod(shape))
     dist = n + gap
     g = rng(n + batch)

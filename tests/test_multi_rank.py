@@ -31,7 +31,7 @@ def _rank_main(rank, world, port, q):
     import bench
 
     class A:
-        gpus, steps, warmup = world, 1, 0
+        gpus, steps, warmup, batch = world, 1, 0, 2
 
     w, r, _ = bench.dist_setup(A)
     # every rank reports a different time; all see the max
@@ -66,3 +66,10 @@ def test_two_gloo_ranks():
     line = json.loads(out0.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port"
+    assert line["config"] == bench_config_of(2, 2)
+
+
+def bench_config_of(batch, world):
+    sys.path.insert(0, ROOT)
+    import bench
+    return bench.bench_config(batch, world)

@@ -47,6 +47,41 @@ def test_2d_nd_golden(golden):
             close(O.ifftn(golden[k], shape).reshape(shape), golden["nd_ifftn_" + key])
 
 
+# The oracle's own error against numpy.fft / scipy (pocketfft, FP64): far
+# inside the 1e-12 budget of the GPU parity tests, so a GPU result within
+# 1e-12 of the oracle is within about 1e-12 of an independent FP64 FFT too.
+ORACLE_PIN = 1e-13
+
+
+def test_oracle_pinned_1e13(golden):
+    checked = 0
+    for k in golden:
+        if k.startswith("c2c_in_"):
+            n = int(k.split("_")[-1])
+            assert rel_l2(O.fft(golden[k]), golden["c2c_fft_%d" % n]) <= ORACLE_PIN, ("fft", n)
+            assert rel_l2(O.ifft(golden[k]), golden["c2c_ifft_%d" % n]) <= ORACLE_PIN, ("ifft", n)
+            checked += 2
+        if k.startswith("r_in_"):
+            n = int(k.split("_")[-1])
+            assert rel_l2(O.rfft(golden[k]), golden["r_rfft_%d" % n]) <= ORACLE_PIN, ("rfft", n)
+            assert rel_l2(O.irfft(golden["r_spec_%d" % n], n), golden["r_irfft_%d" % n]) <= ORACLE_PIN, ("irfft", n)
+            checked += 2
+        if k.startswith("r2_in_"):
+            key = k[len("r2_in_"):]
+            r, c = map(int, key.split("x"))
+            got = O.rfft2(golden[k], r, c).reshape(r, c // 2 + 1)
+            assert rel_l2(got, golden["r2_rfft2_" + key]) <= ORACLE_PIN, ("rfft2", key)
+            checked += 1
+        if k.startswith("nd_in_"):
+            key = k[len("nd_in_"):]
+            shape = list(map(int, key.split("x")))
+            assert rel_l2(O.fftn(golden[k], shape).reshape(shape), golden["nd_fftn_" + key]) <= ORACLE_PIN
+            assert rel_l2(O.ifftn(golden[k], shape).reshape(shape), golden["nd_ifftn_" + key]) <= ORACLE_PIN
+            checked += 2
+    assert rel_l2(O.spectrogram(golden["spec_in"], 32, 20, golden["spec_win"], 1.0), golden["spec_out"]) <= ORACLE_PIN
+    assert checked >= 20
+
+
 def test_spectrogram_golden(golden):
     got = O.spectrogram(golden["spec_in"], 32, 20, golden["spec_win"], 1.0)
     close(got, golden["spec_out"])

@@ -38,6 +38,18 @@ def test_noalloc_matches_exec_c2c(prec, n, batch):
             assert err <= TOL[prec], (prec, n, call, inverse, err)
 
 
+def test_noalloc_rejects_wrong_plans():
+    from fft_b200._lib import GOFFT_EINVAL, GOFFT_EUNSUPPORTED, lib
+    from fft_b200.device import DevicePlan
+    x = torch.zeros(1, 64 * 64, dtype=torch.complex128, device="cuda")
+    xp, st = ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    real = DevicePlan("r2c", "f64", [1024])
+    assert lib().gofft_exec_c2c_noalloc(real.handle, xp, xp, 0, st) == GOFFT_EINVAL
+    assert "complex-to-complex" in lib().gofft_last_error().decode()
+    two_d = DevicePlan("c2c", "f64", [64, 64])
+    assert lib().gofft_exec_c2c_noalloc(two_d.handle, xp, xp, 0, st) == GOFFT_EUNSUPPORTED
+
+
 def test_noalloc_rejects_oversized():
     from fft_b200._lib import GOFFT_EINVAL, lib
     from fft_b200.device import DevicePlan
