@@ -1120,6 +1120,11 @@ extern "C" int gofft_set_lanes(int lanes) {
   g_lanes.store(lanes == 0 ? kLanes : lanes);
   return GOFFT_OK;
 }
+extern "C" int gofft_set_tma_pipeline(int on) {
+  set_tma_pipeline(on);
+  return GOFFT_OK;
+}
+extern "C" int gofft_pipeline_status(void) { return pipe_status(true); }
 extern "C" int gofft_set_pipelined(int precision, int64_t n, int op, int on) {
   set_pipe_override(precision, n, op, on);
   return GOFFT_OK;

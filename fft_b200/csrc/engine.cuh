@@ -384,11 +384,23 @@ template <int N, int T, int R, int... Rs> constexpr int ct_maxe_r() {
 // offsets.
 template <int STEP, class C> GF_DEV C &slot(C *b, int i) { return b[spad(i) * STEP]; }
 
+// The barrier between a stage's loads and its stores: the whole CTA, or (in
+// warp-specialised kernels) only the warps that work on the tile.
+struct CtaBar {
+  static GF_DEV void sync() { __syncthreads(); }
+};
+
 // GUARD: some threads of the block sit out the butterflies (c.t beyond the
-// line); every thread still reaches the barriers.
-template <class P, class Op, int N, int T, int NS, int R, int E, bool FG, bool TG, int STEP, bool GUARD>
+// line); every thread still reaches the barriers.  LAND: the inputs come from
+// an unpadded copy of the line at lb (element i at lb[i * STEP], as a bulk
+// copy lands it) instead of the padded layout; the outputs go to the padded
+// layout at sb (the stage reads everything before its barrier, so lb and sb
+// may overlap).
+template <class P, class Op, int N, int T, int NS, int R, int E, bool FG, bool TG, int STEP, bool GUARD,
+          class BAR = CtaBar, bool LAND = false>
 GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &a, const LineCtx &c,
-                     const typename P::tw_t *tw, const float2 *twh, bool cj) {
+                     const typename P::tw_t *tw, const float2 *twh, bool cj,
+                     const typename P::cpx *lb = nullptr) {
   using C = typename P::cpx;
   constexpr int NB = N / R;
   constexpr int PER = (NB + T - 1) / T;
@@ -397,7 +409,15 @@ GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &
   for (int b = 0; b < PER; b++) {
     const int j = c.t + b * T;
     if (EXACT || j < NB) {
-      if constexpr (!FG && NB % 16 == 0) {
+      if constexpr (LAND) {
+        const C *p = lb + j * STEP;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          C x = p[r * NB * STEP];
+          if (cj) x.y = -x.y;
+          v[b * R + r] = x;
+        }
+      } else if constexpr (!FG && NB % 16 == 0) {
         const C *p = &slot<STEP>(sb, j);
 #pragma unroll
         for (int r = 0; r < R; r++) {
@@ -417,7 +437,7 @@ GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &
       }
     }
   }
-  if constexpr (!FG) __syncthreads();
+  if constexpr (!FG) BAR::sync();
 #pragma unroll
   for (int b = 0; b < PER; b++) {
     const int j = c.t + b * T;
@@ -448,13 +468,13 @@ GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &
       }
     }
   }
-  if constexpr (!TG) __syncthreads();
+  if constexpr (!TG) BAR::sync();
 }
 
 template <class P, class Op, int N, int T, int NS, int TO, int E, bool CAN_FG, bool CAN_TG, int STEP, bool GUARD,
-          int R, int... Rs>
+          class BAR, bool LAND, int R, int... Rs>
 GF_DEV void stages_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &a, const LineCtx &c,
-                      bool cj_first, bool fg, bool tg) {
+                      bool cj_first, bool fg, bool tg, const typename P::cpx *lb) {
   using TW = typename P::tw_t;
   constexpr bool FIRST = NS == 1;
   constexpr bool LAST = sizeof...(Rs) == 0;
@@ -463,33 +483,44 @@ GF_DEV void stages_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs 
   const bool cj = FIRST && cj_first;
   constexpr bool F_OK = FIRST && CAN_FG;
   constexpr bool T_OK = LAST && CAN_TG;
-  if constexpr (F_OK && T_OK) {
-    if (fg && tg) stage_ct<P, Op, N, T, NS, R, E, true, true, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
-    else if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
-    else if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
+  if constexpr (FIRST && LAND) {
+    // first stage from the landing copy (never direct from global memory)
+    if constexpr (T_OK) {
+      if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP, GUARD, BAR, true>(v, sb, a, c, tw, twh, cj, lb);
+      else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD, BAR, true>(v, sb, a, c, tw, twh, cj, lb);
+    } else {
+      stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD, BAR, true>(v, sb, a, c, tw, twh, cj, lb);
+    }
+  } else if constexpr (F_OK && T_OK) {
+    if (fg && tg) stage_ct<P, Op, N, T, NS, R, E, true, true, STEP, GUARD, BAR>(v, sb, a, c, tw, twh, cj);
+    else if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP, GUARD, BAR>(v, sb, a, c, tw, twh, cj);
+    else if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP, GUARD, BAR>(v, sb, a, c, tw, twh, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD, BAR>(v, sb, a, c, tw, twh, cj);
   } else if constexpr (F_OK) {
-    if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
+    if (fg) stage_ct<P, Op, N, T, NS, R, E, true, false, STEP, GUARD, BAR>(v, sb, a, c, tw, twh, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD, BAR>(v, sb, a, c, tw, twh, cj);
   } else if constexpr (T_OK) {
-    if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
-    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
+    if (tg) stage_ct<P, Op, N, T, NS, R, E, false, true, STEP, GUARD, BAR>(v, sb, a, c, tw, twh, cj);
+    else stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD, BAR>(v, sb, a, c, tw, twh, cj);
   } else {
-    stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD>(v, sb, a, c, tw, twh, cj);
+    stage_ct<P, Op, N, T, NS, R, E, false, false, STEP, GUARD, BAR>(v, sb, a, c, tw, twh, cj);
   }
   if constexpr (!LAST)
-    stages_ct<P, Op, N, T, NS * R, TO + NS * (R - 1), E, CAN_FG, CAN_TG, STEP, GUARD, Rs...>(v, sb, a, c, cj_first,
-                                                                                             fg, tg);
+    stages_ct<P, Op, N, T, NS * R, TO + NS * (R - 1), E, CAN_FG, CAN_TG, STEP, GUARD, BAR, LAND, Rs...>(
+        v, sb, a, c, cj_first, fg, tg, lb);
 }
 
 // Runs the compiled schedule on the line at shared-memory base sb; STEP is
-// the element step of the layout (1: row layout, LPC: column layout).
-template <class P, class Op, int N, int T, bool CAN_FG, bool CAN_TG, int STEP, bool GUARD = false, int... Rs>
+// the element step of the layout (1: row layout, LPC: column layout).  BAR is
+// the stages' barrier; LAND makes the first stage read the unpadded landing
+// copy at lb.
+template <class P, class Op, int N, int T, bool CAN_FG, bool CAN_TG, int STEP, bool GUARD = false,
+          class BAR = CtaBar, bool LAND = false, int... Rs>
 GF_DEV void run_stages_ct(Sched<Rs...>, typename P::cpx *sb, const KArgs &a, const LineCtx &c, bool cj_first,
-                          bool fg, bool tg) {
+                          bool fg, bool tg, const typename P::cpx *lb = nullptr) {
   constexpr int E = ct_maxe_r<N, T, Rs...>();
   typename P::cpx v[E];
-  stages_ct<P, Op, N, T, 1, 0, E, CAN_FG, CAN_TG, STEP, GUARD, Rs...>(v, sb, a, c, cj_first, fg, tg);
+  stages_ct<P, Op, N, T, 1, 0, E, CAN_FG, CAN_TG, STEP, GUARD, BAR, LAND, Rs...>(v, sb, a, c, cj_first, fg, tg, lb);
 }
 
 }  // namespace gf

@@ -5,6 +5,11 @@
 #include <cstring>
 #include <sstream>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "pipe.h"
+#include "pipe.cuh"
 #include "plan.cuh"
 
 namespace gf {
@@ -580,10 +585,185 @@ int choose_flags(int op, const KArgs &a) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// The TMA-fed persistent line kernel (k_pipe, pipe.cuh), for the plain
+// complex, packed real forward and packed real inverse lines whenever an
+// instance was built for the line's schedule and the layout suits it.  Off by
+// default (gofft_set_tma_pipeline turns it on): on the 1024 x 1024 real round
+// trip it measured no faster per launch than the one-tile-per-CTA kernels
+// (its warps wait at the stage barriers instead of on the first stage's
+// loads), and its one CTA per SM keeps the next L2 block's launch from
+// overlapping the tail of the current one.
+// ---------------------------------------------------------------------------
+static std::atomic<int> g_pipe_on{0};
+void set_tma_pipeline(int on) { g_pipe_on.store(on ? 1 : 0); }
+int tma_pipeline() { return g_pipe_on.load(); }
+
+// The kernels' timeout word (set when a bounded wait gives up), one per
+// device in the library image: its address comes from cudaGetSymbolAddress,
+// so using it allocates nothing.
+static __device__ int g_pipe_err;
+static std::mutex g_pipe_err_mu;
+static std::map<int, int *> g_pipe_err_addr;
+static int *pipe_err_word() {
+  const int d = cur_device();
+  std::lock_guard<std::mutex> lk(g_pipe_err_mu);
+  auto it = g_pipe_err_addr.find(d);
+  if (it != g_pipe_err_addr.end()) return it->second;
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_pipe_err) != cudaSuccess) return nullptr;
+  g_pipe_err_addr[d] = (int *)p;
+  return (int *)p;
+}
+int pipe_status(bool clear) {
+  int *w = pipe_err_word();
+  if (!w) return set_err(3, "pipeline status word unavailable");
+  int v = 0;
+  GF_CK(cudaDeviceSynchronize());
+  GF_CK(cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost));
+  if (v && clear) {
+    const int zero = 0;
+    GF_CK(cudaMemcpy(w, &zero, sizeof(int), cudaMemcpyHostToDevice));
+  }
+  return v ? set_err(4, "a pipelined line kernel's wait timed out") : 0;
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
+
+static PipeInst pipe_instance(const DevProg &dp, int op, bool col) {
+  const int *r = dp.lp.radix;
+  switch (dp.prec) {
+    case F64: return pipe_kernel_f64(op, dp.n, dp.lp.T, r, dp.lp.nst, col);
+    case F32: return pipe_kernel_f32(op, dp.n, dp.lp.T, r, dp.lp.nst, col);
+    default: return pipe_kernel_f32c(op, dp.n, dp.lp.T, r, dp.lp.nst, col);
+  }
+}
+
+// Launches the line op on k_pipe when it applies: 1 (status in *rc) if it
+// did, 0 when the caller should use the other line kernels.
+static int try_pipe(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st, int *rc) {
+  if (!g_pipe_on.load()) return 0;
+  if (op != OP_C2C && op != OP_R2C && op != OP_C2R) return 0;
+  const int n = dp.n;
+  if (n < 16 || dp.lp.nst == 0) return 0;
+  const size_t E = csize(dp.prec);
+  bool col = false;
+  if (op == OP_C2C) {
+    col = side_col(a.in);
+    if (col != side_col(a.out)) return 0;
+    if (!col && (a.in.stride != 1 || a.out.stride != 1)) return 0;
+  } else if (op == OP_R2C) {
+    if (a.in.stride != 1 || !(a.ic & GF_PAIR_ALIGNED)) return 0;
+  } else {
+    if (a.in.stride != 1 || !(a.ic & GF_PAIR_ALIGNED) || (a.ic & GF_IC_MASK) != n + 1) return 0;
+  }
+  // the last stage indexes a line with 32-bit element offsets
+  if (std::max(std::llabs(a.in.stride), std::llabs(a.out.stride)) * (long long)n >= (1ll << 31)) return 0;
+  const PipeInst pi = pipe_instance(dp, op, col);
+  if (!pi.fn || pi.smem > max_smem_optin()) return 0;
+  PipeArgs pa{};
+  pa.err = pipe_err_word();
+  if (!pa.err) return 0;
+  pa.spin_limit = 1u << 24;
+  CUtensorMap map;
+  memset(&map, 0, sizeof(map));
+  const int L = pi.lpc;
+  if (col) {
+    // lines are the columns of images: line b * ncols + c, adjacent columns
+    // adjacent in memory
+    const long long ncols = a.in.lpb.d;
+    if (a.in.dist_l != 1 || a.in.boff || nlines % ncols != 0) return 0;
+    const long long nimg = nlines / ncols;
+    pa.ncols = (int)ncols;
+    pa.tpb = (int)((ncols + L - 1) / L);
+    pa.ntiles = nimg * pa.tpb;
+    const int BR = n <= 256 ? n : 256;
+    pa.box_rows = BR;
+    pa.fill = PIPE_COL_ASYNC;
+    // 2-D tensor copies when the images are the stacked rows of one array
+    // whose row pitch and base meet the 16-byte rule
+    const long long rows = nimg * n;
+    auto enc = tensor_map_encoder();
+    if (enc && a.in.dist_b == (long long)n * a.in.stride && n % BR == 0 && ((uintptr_t)a.in.ptr % 16) == 0 &&
+        ((size_t)a.in.stride * E) % 16 == 0 && rows < (1ll << 31) && 2 * ncols < (1ll << 31)) {
+      const cuuint64_t dims[2] = {(cuuint64_t)(2 * ncols), (cuuint64_t)rows};
+      const cuuint64_t strides[1] = {(cuuint64_t)(a.in.stride * E)};
+      const cuuint32_t box[2] = {(cuuint32_t)(2 * L), (cuuint32_t)BR};
+      const cuuint32_t estr[2] = {1, 1};
+      const CUresult r = enc(&map, dp.prec == F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                             2, a.in.ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r == CUDA_SUCCESS) pa.fill = PIPE_COL_TMA;
+    }
+  } else {
+    pa.lp = op == OP_C2R ? n + 1 : n;
+    pa.ntiles = (nlines + L - 1) / L;
+    long long D = 0;
+    pa.span = side_simple(a.in, D) ? D : 0;
+    pa.fill = ((uintptr_t)a.in.ptr % 16) == 0 ? PIPE_ROW_BULK : PIPE_ROW_ASYNC;
+  }
+  // a persistent CTA pays off when it has tiles to overlap: with fewer than
+  // two per SM the one-tile-per-CTA kernels fill the GPU better
+  if (pa.ntiles < 2ll * num_sms()) return 0;
+  a.lp = dp.lp;
+  a.nlines = nlines;
+  a.lpc = L;
+  a.ndiv = FastDiv((uint32_t)n);
+  a.lpcdiv = FastDiv((uint32_t)L);
+  a.flags = (col ? GF_COLMAP : 0) | GF_LAST_DIRECT;
+  if (int e = ensure_smem((KFn)pi.fn, pi.smem)) {
+    *rc = e;
+    return 1;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pi.fn, pi.threads, pi.smem);
+  if (per_sm < 1) per_sm = 1;
+  const long long grid = std::min<long long>(pa.ntiles, (long long)per_sm * num_sms());
+  typedef void (*PipeFn)(KArgs, PipeArgs, CUtensorMap);
+  count_launch();
+  TimingRec rec;
+  const bool timed = g_timing.load() != 0;
+  if (timed) {
+    cudaEventCreate(&rec.a);
+    cudaEventCreate(&rec.b);
+    cudaEventRecord(rec.a, st);
+  }
+  ((PipeFn)pi.fn)<<<(unsigned)grid, pi.threads, pi.smem, st>>>(a, pa, map);
+  const cudaError_t e = cudaGetLastError();
+  if (timed) {
+    cudaEventRecord(rec.b, st);
+    std::ostringstream k;
+    k << op_name(op) << "/n=" << n << "/prec=" << dp.prec << "/pipe/lpc=" << L << "/T=" << dp.lp.T
+      << "/fill=" << pa.fill;
+    rec.key = k.str();
+    rec.bytes = algo_bytes(op, dp, a, nlines);
+    std::lock_guard<std::mutex> lk(g_tmu);
+    g_trecs.push_back(rec);
+  }
+  *rc = e == cudaSuccess ? 0 : set_err(3, std::string("pipelined line kernel: ") + cudaGetErrorString(e));
+  return 1;
+}
+
 int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st, int lpc,
                 bool conv) {
   if (nlines <= 0) return 0;
   if (nlines >= (1ll << 31)) return set_err(5, "too many lines in one launch");
+  if (!conv && lpc <= 0) {
+    int rc = 0;
+    if (try_pipe(op, dp, a, nlines, st, &rc)) return rc;
+  }
   a.lp = dp.lp;
   a.nlines = nlines;
   if (lpc <= 0) lpc = choose_lpc(dp, a, op, nlines, conv);

@@ -167,6 +167,13 @@ inline Side mk_side(void *p, long long dist_b, long long dist_l, long long strid
 // Contiguous lines of length len.
 inline Side contig(void *p, long long len) { return mk_side(p, len, 0, 1, 1); }
 
+// The TMA-fed persistent line kernel: on (default) or off for plain complex
+// and packed real lines; pipe_status reads (and with clear, resets) the
+// device's timeout word: 0, or 4 (timeout) with the error text set.
+void set_tma_pipeline(int on);
+int tma_pipeline();
+int pipe_status(bool clear);
+
 // Instrumentation (launch counter, CUDA-event timing per line kernel).
 void count_launch();
 long long launch_count();

@@ -70,3 +70,16 @@ def set_lanes(lanes):
     """Streams plans created afterwards rotate their L2 blocks over: 2 (the
     default; 0 restores it) or 1 (blocks back to back, each pass alone)."""
     check(lib().gofft_set_lanes(int(lanes)))
+
+
+def set_tma_pipeline(on):
+    """The TMA-fed persistent line kernel on or off (the default) for
+    launches made afterwards (results agree to rounding; a comparison
+    switch)."""
+    check(lib().gofft_set_tma_pipeline(1 if on else 0))
+
+
+def pipeline_status():
+    """Raises if a pipelined line kernel's bounded wait gave up since the
+    last call (synchronises the device)."""
+    check(lib().gofft_pipeline_status())

@@ -324,6 +324,19 @@ GOFFT_API int gofft_set_l2_block_bytes(int64_t bytes);
  * next block's; 1 runs the blocks one after another on the caller's stream
  * (each pass then runs alone, e.g. to time it).  GOFFT_EINVAL otherwise. */
 GOFFT_API int gofft_set_lanes(int lanes);
+/* Turns the TMA-fed persistent line kernel on (1) or off (0, the default)
+ * for launches made afterwards.  When on, plain complex lines and the packed
+ * real lines of even-length real transforms run on it wherever an instance
+ * was built for the line's schedule: tiles are copied into a ring of
+ * shared-memory slots (tensor copies for image columns, bulk copies for rows)
+ * while the CTA's warp groups transform earlier tiles.  Results agree with
+ * the default kernels to rounding (a tuning and comparison switch). */
+GOFFT_API int gofft_set_tma_pipeline(int on);
+/* Reads and clears the current device's timeout word of the pipelined line
+ * kernel (synchronises the device): GOFFT_OK, or GOFFT_ETIMEOUT if one of its
+ * bounded waits gave up since the last call (results of that launch are
+ * then invalid).  No such wait gives up in normal operation. */
+GOFFT_API int gofft_pipeline_status(void);
 /* Selects (on = 1) the persistent double-buffered line kernel for
  * (precision, n, op) where one exists.  Used by the autotuner. */
 GOFFT_API int gofft_set_pipelined(int precision, int64_t n, int op, int on);

@@ -164,6 +164,6 @@ def test_timeout_drains_at_default_limit():
         return dt, d["phase_list"][-1]["tiles"], d["grid"]
 
     t_one, tiles_one, grid = timed([65536, 128])
-    t_many, tiles_many, _ = timed([65536] * 48 + [128])
+    t_many, tiles_many, _ = timed([65536] * 160 + [128])
     assert tiles_one <= grid and tiles_many >= 4 * grid, (tiles_one, tiles_many, grid)
     assert t_many < 2.0 * t_one + 1.0, (t_one, t_many)

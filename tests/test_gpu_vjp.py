@@ -127,6 +127,8 @@ def test_filter2_workload_vs_oracle(prec, c5):
 # relative part of the finite-difference tolerance, and the unit roundoff
 FD_RTOL = {"f64": 1e-6, "f32mixed": 2e-2, "f32": 2e-2}
 FD_U = {"f64": 2.0 ** -53, "f32mixed": 2.0 ** -24, "f32": 2.0 ** -24}
+# rounding floor of the central differences, in units of u L' / h (see fd_check)
+FD_FLOOR = 16
 
 
 def fd_check(f, xt, Ht, y, dx, dH, eps, rtol, u, seed=24, n_x=32, n_h=32):
@@ -137,13 +139,14 @@ def fd_check(f, xt, Ht, y, dx, dH, eps, rtol, u, seed=24, n_x=32, n_h=32):
     engine's outputs (images the step leaves alone are bitwise equal and
     cancel).  L is quadratic, so the central difference is exact for every
     step and what remains is rounding.  Tolerance per coordinate: the
-    textbook floor of a difference quotient, 4 u L' / h (u the unit roundoff,
-    L' the part of L the step changes, h the step), plus rtol |gradient|.
-    The floor is conservative: L(+) - L(-) sums the products of N output
-    differences, whose independent roundings grow like sqrt(N) u L', far
-    below 4 u L'.  In FP32 the floor exceeds the x gradients of 512 x 512
-    images (L' is about 6.6e4 per image for a step of 2e-3): there the check
-    is a bound, and the callers add closeness checks on the coordinates whose
+    rounding floor of a difference quotient, FD_FLOOR u L' / h (u the unit
+    roundoff, L' the part of L the step changes, h the step), plus
+    rtol |gradient|.  The rounding of L(+) - L(-) was measured at up to
+    4.7 u L' on this workload (FP64, x coordinate (3, 308, 366) of seed 24:
+    2.07e-6 against a gradient of 0.038 at h = 2e-6, L' = 7934), so the floor
+    is 16 u L' / h, about three times that.  In FP32 the floor exceeds the x
+    gradients of 512 x 512 images (L' is about 6.6e4 per image for a step of
+    2e-3): there the check is a bound, and the callers add closeness checks on the coordinates whose
     gradients stand well above it.  The difference at 2 eps is evaluated as
     well and held to the same bound (the gradient must not depend on the
     step)."""
@@ -180,16 +183,16 @@ def fd_check(f, xt, Ht, y, dx, dH, eps, rtol, u, seed=24, n_x=32, n_h=32):
         b, i, j = (int(v) for v in (g.integers(0, B), g.integers(0, R), g.integers(0, C)))
         a1, a2 = fd_x(b, i, j, eps), fd_x(b, i, j, 2 * eps)
         want = float(dx[b, i, j])
-        assert abs(a1 - want) <= 4 * u * L_img[b] / (2 * eps) + rtol * abs(want), ("x", b, i, j, a1, want)
-        assert abs(a2 - want) <= 4 * u * L_img[b] / (4 * eps) + rtol * abs(want), ("x2", b, i, j, a2, want)
+        assert abs(a1 - want) <= FD_FLOOR * u * L_img[b] / (2 * eps) + rtol * abs(want), ("x", b, i, j, a1, want)
+        assert abs(a2 - want) <= FD_FLOOR * u * L_img[b] / (4 * eps) + rtol * abs(want), ("x2", b, i, j, a2, want)
         checked.append((abs(want), abs(a1 - want) / (abs(want) + 1e-300)))
     for q in range(n_h):
         r, k = int(g.integers(0, R)), int(g.integers(0, K))
         unit = 1.0 if q % 2 == 0 else 1j
         a1, a2 = fd_h(r, k, unit, eps), fd_h(r, k, unit, 2 * eps)
         want = float(dH[r, k].real if unit == 1.0 else dH[r, k].imag)
-        assert abs(a1 - want) <= 4 * u * L_all / (2 * eps) + rtol * abs(want), ("H", r, k, unit, a1, want)
-        assert abs(a2 - want) <= 4 * u * L_all / (4 * eps) + rtol * abs(want), ("H2", r, k, unit, a2, want)
+        assert abs(a1 - want) <= FD_FLOOR * u * L_all / (2 * eps) + rtol * abs(want), ("H", r, k, unit, a1, want)
+        assert abs(a2 - want) <= FD_FLOOR * u * L_all / (4 * eps) + rtol * abs(want), ("H2", r, k, unit, a2, want)
         checked.append((abs(want), abs(a1 - want) / (abs(want) + 1e-300)))
     return checked
 
