@@ -20,7 +20,8 @@ enum Op {
   OP_RADER_FS2 = 10,  // two-pass Rader: row pass with spectrum multiply
   OP_RADER_FS4 = 11,  // two-pass Rader: row pass with the output scatter
   OP_FILTER_COL = 12, // 2-D spectral filter: column FFT, multiply, column IFFT
-  OP_COUNT = 13
+  OP_RADER_IP = 13,   // Rader with the whole convolution in shared memory (rader_ip.cuh)
+  OP_COUNT = 14
 };
 
 typedef void (*KFn)(KArgs);
@@ -89,6 +90,11 @@ cudaError_t gen_rader_kernel(double2 *b, const int *perm, long long p, long long
                              cudaStream_t st);
 cudaError_t gen_chirp(long long *jj, double2 *w, long long n, cudaStream_t st);
 cudaError_t gen_blue_kernel(double2 *b, const double2 *w, long long n, long long m, cudaStream_t st);
+// The in-shared-memory Rader kernel (k_rader_ip) of each precision and its
+// threads per CTA.
+const void *rader_ip_kernel_f64(int *threads);
+const void *rader_ip_kernel_f32(int *threads);
+const void *rader_ip_kernel_f32c(int *threads);
 // The persistent multi-phase kernel (k_persist) of each precision.
 const void *persist_kernel_f64();
 const void *persist_kernel_f32();

@@ -1,0 +1,8 @@
+// k_rip_f64.cu -- in-shared-memory Rader kernel (PrecF64).
+#include "rader_ip.cuh"
+namespace gf {
+const void *rader_ip_kernel_f64(int *threads) {
+  *threads = rip_threads<PrecF64>();
+  return (const void *)k_rader_ip<PrecF64>;
+}
+}  // namespace gf

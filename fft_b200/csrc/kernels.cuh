@@ -4,6 +4,7 @@
 #include <type_traits>
 #include "dispatch.h"
 #include "ops.cuh"
+#include "rader_ip.cuh"
 
 namespace gf {
 
@@ -124,6 +125,13 @@ __device__ __noinline__ void persist_line_body(const KArgs &a, long long tile, b
   line_body<P, 16, Op>(a, tile, active);
 }
 
+// One signal of an in-shared-memory Rader phase (one line per item; every
+// thread of the CTA works on it).
+template <class P>
+__device__ __noinline__ void persist_rip_body(const KArgs &a, long long line) {
+  if (line < a.nlines) rader_ip_line<P>(a, line);
+}
+
 template <class P>
 GF_DEV void phase_dispatch(const KArgs &a, int op, long long tile, bool active) {
   if ((op == OP_C2C || op == OP_C2C_TW) && persist_ct<P>(a, op, tile, active)) return;
@@ -135,6 +143,7 @@ GF_DEV void phase_dispatch(const KArgs &a, int op, long long tile, bool active) 
     case OP_RADER_FS1: persist_line_body<P, OpRaderFS1>(a, tile, active); break;
     case OP_RADER_FS2: persist_line_body<P, OpRaderFS2>(a, tile, active); break;
     case OP_RADER_FS4: persist_line_body<P, OpRaderFS4>(a, tile, active); break;
+    case OP_RADER_IP: persist_rip_body<P>(a, tile); break;
     default: break;
   }
 }

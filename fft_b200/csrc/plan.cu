@@ -11,6 +11,7 @@
 #include "pipe.h"
 #include "pipe.cuh"
 #include "plan.cuh"
+#include "rader_ip.cuh"
 
 namespace gf {
 
@@ -438,7 +439,7 @@ std::string timing_report() {
 static const char *op_name(int op) {
   static const char *n[] = {"c2c", "c2c_twiddle", "r2c_packed", "c2r_packed", "r2c_full", "c2r_full",
                             "rader_fused", "bluestein_fused", "spectrogram", "rader_fs1", "rader_fs2",
-                            "rader_fs4", "filter_col"};
+                            "rader_fs4", "filter_col", "rader_inplace"};
   return (op >= 0 && op < OP_COUNT) ? n[op] : "?";
 }
 
@@ -451,6 +452,7 @@ static double algo_bytes(int op, const DevProg &dp, const KArgs &a, long long nl
     case OP_R2C_FULL:
     case OP_C2R_FULL: return nl * (n * r + (double)(dp.n / 2 + 1) * c);
     case OP_RADER:
+    case OP_RADER_IP:
     case OP_BLUE: return 2.0 * nl * (double)a.ia * c;
     case OP_SPECTRO: return nl * (2 * n * r + (n + 1) * r);
     case OP_FILTER_COL: {
@@ -756,10 +758,51 @@ static int try_pipe(int op, const DevProg &dp, KArgs a, long long nlines, cudaSt
   return 1;
 }
 
+// The in-shared-memory Rader kernel: one CTA per signal (persistent over the
+// signals), the convolution of length dp.n in dynamic shared memory.
+static int launch_rader_ip(const DevProg &dp, KArgs a, long long nlines, cudaStream_t st) {
+  int threads = 0;
+  const void *f = dp.prec == F64 ? rader_ip_kernel_f64(&threads)
+                                 : (dp.prec == F32 ? rader_ip_kernel_f32(&threads) : rader_ip_kernel_f32c(&threads));
+  a.lp = dp.lp;
+  a.nlines = nlines;
+  a.lpc = 1;
+  a.ndiv = FastDiv((uint32_t)dp.n);
+  a.lpcdiv = FastDiv(1);
+  a.flags = 0;
+  const size_t smem = (size_t)dp.n * csize(dp.prec);
+  if (int rc = ensure_smem((KFn)f, smem)) return rc;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, threads, smem);
+  if (per_sm < 1) return set_err(5, "in-place Rader kernel does not fit an SM");
+  const long long grid = std::min<long long>(nlines, (long long)per_sm * num_sms());
+  count_launch();
+  TimingRec rec;
+  const bool timed = g_timing.load() != 0;
+  if (timed) {
+    cudaEventCreate(&rec.a);
+    cudaEventCreate(&rec.b);
+    cudaEventRecord(rec.a, st);
+  }
+  ((KFn)f)<<<(unsigned)grid, threads, smem, st>>>(a);
+  GF_CK(cudaGetLastError());
+  if (timed) {
+    cudaEventRecord(rec.b, st);
+    std::ostringstream k;
+    k << op_name(OP_RADER_IP) << "/p=" << a.ia << "/cl=" << dp.n << "/prec=" << dp.prec << "/T=" << threads;
+    rec.key = k.str();
+    rec.bytes = algo_bytes(OP_RADER_IP, dp, a, nlines);
+    std::lock_guard<std::mutex> lk(g_tmu);
+    g_trecs.push_back(rec);
+  }
+  return 0;
+}
+
 int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream_t st, int lpc,
                 bool conv) {
   if (nlines <= 0) return 0;
   if (nlines >= (1ll << 31)) return set_err(5, "too many lines in one launch");
+  if (op == OP_RADER_IP) return launch_rader_ip(dp, a, nlines, st);
   if (!conv && lpc <= 0) {
     int rc = 0;
     if (try_pipe(op, dp, a, nlines, st, &rc)) return rc;
@@ -831,7 +874,7 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
 // Exec1D
 // ---------------------------------------------------------------------------
 Exec1D::~Exec1D() {
-  for (void *p : {(void *)tw4, (void *)perm, (void *)iperm, (void *)jj, spec, chirp})
+  for (void *p : {(void *)tw4, (void *)perm, (void *)iperm, (void *)jj, spec, chirp, spec_ip})
     if (p) cudaFree(p);
 }
 
@@ -840,7 +883,7 @@ size_t Exec1D::ws_bytes(long long nl) const {
   switch (kind) {
     case K_FOURSTEP: return 3 * (size_t)n * nl * c + 256;
     case K_RADER:
-      if (fused) return 0;
+      if (fused || inplace) return 0;
       return (2 * (size_t)n + 2 * (size_t)cl + 2) * nl * c + 1024;
     case K_BLUE:
       if (fused) return 0;
@@ -931,6 +974,20 @@ int Exec1D::exec(const Side &in, const Side &out, long long nl, int cji, int cjo
         a.ia = n;
         a.ic = cyclic ? 0 : (int)(n - 1);
         return launch_line(OP_RADER, *prog, a, nl, st, 0, true);
+      }
+      if (inplace) {
+        KArgs a{};
+        a.in = in;
+        a.out = out;
+        a.cj_in = cji;
+        a.cj_out = cjo;
+        a.scale = scale;
+        a.aux0 = perm;
+        a.aux1 = iperm;
+        a.aux2 = spec_ip;
+        a.ia = n;
+        a.ic = cyclic ? 0 : (int)(n - 1);
+        return launch_line(OP_RADER_IP, *ipprog, a, nl, st);
       }
       return rader_two_pass(in, out, nl, cji, cjo, scale, ws, st);
     }
@@ -1096,7 +1153,9 @@ std::string Exec1D::describe() const {
   };
   if (kind == K_SINGLE && prog) o << ",\"prog\":" << sched(*prog);
   if (kind == K_FOURSTEP) o << ",\"n1\":" << n1 << ",\"n2\":" << n2 << ",\"p1\":" << sched(*p1) << ",\"p2\":" << sched(*p2);
-  if (kind == K_RADER) o << ",\"g\":" << g << ",\"cl\":" << cl << ",\"cyclic\":" << cyclic << ",\"fused\":" << (fused ? 1 : 0);
+  if (kind == K_RADER)
+    o << ",\"g\":" << g << ",\"cl\":" << cl << ",\"cyclic\":" << cyclic << ",\"fused\":" << (fused ? 1 : 0)
+      << ",\"inplace\":" << (inplace ? 1 : 0);
   if (kind == K_BLUE) o << ",\"m\":" << m << ",\"fused\":" << (fused ? 1 : 0);
   if ((kind == K_RADER || kind == K_BLUE) && fused && prog) o << ",\"prog\":" << sched(*prog);
   if ((kind == K_RADER || kind == K_BLUE) && !fused && sub) o << ",\"conv\":" << sub->describe();
@@ -1124,6 +1183,65 @@ static int make_spectrum(int prec, double2 *b, long long L, void **spec_out) {
   cudaFree(B);
   if (ws) cudaFree(ws);
   return rc;
+}
+
+// In-shared-memory Rader (rader_ip.cuh) for a convolution of length ex.cl
+// that fits one CTA's shared memory: the stage list in decimation-in-
+// frequency order (radix R_s, stride S_s = cl / (R_0 ... R_s)), the twiddle
+// planes W_{R S}^{j m} (j < S, the Stockham table layout with ns = S), and
+// the kernel spectrum permuted to the digit-reversed order the forward stages
+// leave: A[k] at pos = sum_s m_s S_s for k = m_0 + R_0 m_1 + R_0 R_1 m_2 + ...
+// Returns 0 when built, 1 when the length does not qualify, else an error.
+static int build_rader_ip(Exec1D &ex) {
+  const long long cl = ex.cl;
+  const int prec = ex.prec;
+  if ((size_t)cl * csize(prec) > max_smem_optin()) return 1;
+  const std::vector<int> rad = gpu_radices(cl, 3);
+  if (rad.empty() || (int)rad.size() > GF_MAXST) return 1;
+  for (int R : rad)
+    if (!rip_radix_ok(R)) return 1;
+  auto dp = std::make_shared<DevProg>();
+  dp->n = (int)cl;
+  dp->prec = prec;
+  dp->device = cur_device();
+  LineProg &lp = dp->lp;
+  lp.n = (int)cl;
+  lp.nst = (int)rad.size();
+  lp.T = 1;
+  lp.maxe = 16;
+  StageTab tab{};
+  tab.nst = lp.nst;
+  long long S = cl, off = 0;
+  for (int s = 0; s < lp.nst; s++) {
+    S /= rad[s];
+    lp.radix[s] = tab.radix[s] = rad[s];
+    lp.ns[s] = tab.ns[s] = (int)S;
+    lp.twoff[s] = tab.twoff[s] = (int)off;
+    lp.nsdiv[s] = FastDiv((uint32_t)S);
+    off += S * (rad[s] - 1);
+  }
+  GF_CK(cudaMalloc(&dp->tw, std::max<long long>(off, 1) * twsize(prec)));
+  lp.tw = dp->tw;
+  if (off > 0) GF_CK(GF_PREC_CALL(prec, stage_tw, dp->tw, tab, off, 0));
+  // the spectrum in digit-reversed order (16-byte entries in every precision)
+  std::vector<unsigned char> h((size_t)cl * 16), hp((size_t)cl * 16);
+  GF_CK(cudaMemcpy(h.data(), ex.spec, h.size(), cudaMemcpyDeviceToHost));
+  for (long long pos = 0; pos < cl; pos++) {
+    long long rem = pos, k = 0, mult = 1;
+    for (int s = 0; s < lp.nst; s++) {
+      const long long m = rem / lp.ns[s];
+      rem -= m * lp.ns[s];
+      k += m * mult;
+      mult *= lp.radix[s];
+    }
+    memcpy(&hp[(size_t)pos * 16], &h[(size_t)k * 16], 16);
+  }
+  GF_CK(cudaMalloc(&ex.spec_ip, hp.size()));
+  GF_CK(cudaMemcpy(ex.spec_ip, hp.data(), hp.size(), cudaMemcpyHostToDevice));
+  GF_CK(cudaStreamSynchronize(0));
+  ex.ipprog = dp;
+  ex.inplace = true;
+  return 0;
 }
 
 static int build_exec(long long n, int prec, std::shared_ptr<Exec1D> &out) {
@@ -1185,6 +1303,8 @@ static int build_exec(long long n, int prec, std::shared_ptr<Exec1D> &out) {
       ex->prog = conv->prog;
     } else {
       ex->sub = conv;
+      const int r = build_rader_ip(*ex);
+      if (r > 1) return r;
     }
     out = ex;
     return 0;

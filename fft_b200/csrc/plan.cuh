@@ -91,6 +91,12 @@ struct Exec1D {
   long long n1 = 0, n2 = 0;
   void *tw4 = nullptr;                  // FOURSTEP: W_n^e, e < n
   bool fused = false;
+  // Rader whose convolution fits one CTA's shared memory but not the
+  // register-staged line kernels: the in-place kernel (rader_ip.cuh), with
+  // its stage list in ipprog and the kernel spectrum in digit-reversed order
+  bool inplace = false;
+  std::shared_ptr<DevProg> ipprog;
+  void *spec_ip = nullptr;
   long long cl = 0, g = 0, m = 0;
   int cyclic = 0;
   int *perm = nullptr, *iperm = nullptr;

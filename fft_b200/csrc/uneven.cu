@@ -4,7 +4,8 @@
 // The signals are grouped by length.  Each length's executor is lowered to a
 // list of phases (one line op over a number of tiles): one phase for a length
 // that fits one CTA (and for a Rader or Bluestein transform whose convolution
-// fits one CTA), two for the four-step split, four for Rader over a two-pass
+// fits one CTA, and for a Rader transform whose convolution fits one CTA's
+// shared memory), two for the four-step split, four for Rader over a two-pass
 // convolution.  Phases are ordered by dependency level (every first phase,
 // then every second phase, ...) and executed by k_persist, whose CTAs claim
 // (phase, tile) items from a counter; a phase waits, with a bounded spin, for
@@ -116,7 +117,8 @@ static int add_class(gofft_uneven *u, gofft_uneven::Cls &c, size_t *wsoff, std::
     PhaseDesc p{};
     a.lp = prog->lp;
     a.nlines = nlines;
-    a.lpc = choose_lpc(*prog, a, op, nlines, conv);
+    // the in-shared-memory Rader works on one signal per item
+    a.lpc = op == OP_RADER_IP ? 1 : choose_lpc(*prog, a, op, nlines, conv);
     a.ndiv = FastDiv((uint32_t)prog->n);
     a.lpcdiv = FastDiv((uint32_t)a.lpc);
     a.flags = choose_flags(op, a) & GF_COLMAP;
@@ -177,6 +179,19 @@ static int add_class(gofft_uneven *u, gofft_uneven::Cls &c, size_t *wsoff, std::
     a.aux2 = e.spec;
     a.ia = e.n;
     push(OP_BLUE, e.prog, a, cnt, -1, 0, true);
+    return 0;
+  }
+  if (e.kind == K_RADER && e.inplace) {
+    KArgs a{};
+    a.in = in1;
+    a.out = out1;
+    a.scale = 1.0;
+    a.aux0 = e.perm;
+    a.aux1 = e.iperm;
+    a.aux2 = e.spec_ip;
+    a.ia = e.n;
+    a.ic = e.cyclic ? 0 : (int)(e.n - 1);
+    push(OP_RADER_IP, e.ipprog, a, cnt, -1, 0, false);
     return 0;
   }
   if (e.kind == K_RADER && e.sub && e.sub->kind == K_FOURSTEP) {
@@ -259,10 +274,12 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
     return u->cls[x].n * (long long)u->cls[x].sig.size() > u->cls[y].n * (long long)u->cls[y].sig.size();
   });
   std::vector<int> cls_lane(u->cls.size()), raw_lane;
+  std::vector<long long> raw_len;  // class length of each phase
   for (size_t r = 0; r < by_size.size(); r++) cls_lane[by_size[r]] = (int)(r % gofft_uneven::kLanes);
   for (size_t ci = 0; ci < u->cls.size(); ci++) {
     if (int rc = add_class(u.get(), u->cls[ci], &wsoff, raw, lvl, progs)) return rc;
     raw_lane.resize(raw.size(), cls_lane[ci]);
+    raw_len.resize(raw.size(), u->cls[ci].n);
   }
   // order by level, keeping class order within a level; remap dependencies
   std::vector<int> order(raw.size());
@@ -307,28 +324,19 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
       p.a.scale = 1.0;  // set below per class length
     }
   }
-  // scale 1/n on the last phase of each class: find the class length by walking
-  // the class order (phases of a class share the executor length)
-  {
-    size_t k = 0;
-    std::vector<long long> len_of(raw.size());
-    for (auto &c : u->cls) {
-      const Exec1D &e = *c.ex;
-      int np = e.kind == K_FOURSTEP ? 2 : (e.kind == K_RADER && !e.fused ? 4 : 1);
-      for (int t = 0; t < np; t++) len_of[k++] = c.n;
-    }
-    for (int i = 0; i < u->nph; i++) {
-      bool has_child = false;
-      for (int j = 0; j < u->nph; j++)
-        if (u->ph[1][j].dep == i) has_child = true;
-      if (!has_child) u->ph[1][i].a.scale = 1.0 / (double)len_of[order[i]];
-    }
+  // scale 1/n on the last phase of each class (n its class length)
+  for (int i = 0; i < u->nph; i++) {
+    bool has_child = false;
+    for (int j = 0; j < u->nph; j++)
+      if (u->ph[1][j].dep == i) has_child = true;
+    if (!has_child) u->ph[1][i].a.scale = 1.0 / (double)raw_len[order[i]];
   }
   // launch shape: enough threads and shared memory for every phase
   for (int i = 0; i < u->nph; i++) {
     const PhaseDesc &p = u->ph[0][i];
     const bool conv = p.op == OP_RADER || p.op == OP_BLUE;
-    u->block = std::max(u->block, p.a.lpc * p.a.lp.T);
+    // an in-shared-memory Rader item runs on every thread of the CTA
+    u->block = std::max(u->block, p.op == OP_RADER_IP ? 512 : p.a.lpc * p.a.lp.T);
     u->smem = std::max(u->smem, (size_t)p.a.lpc * spad_size(p.a.lp.n) * csize(precision) +
                                     (conv ? 2 * p.a.lpc * csize(precision) : 0));
   }
@@ -343,6 +351,9 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
   for (int d = 0; d < 2; d++) GF_CK(cudaMalloc(&u->d_ph[d], u->nph * sizeof(PhaseDesc)));
   GF_CK(cudaMallocHost(&u->h_pinned, u->nph * sizeof(PhaseDesc)));
   GF_CK(cudaMalloc(&u->d_ctr, sizeof(unsigned long long) * (2 + (u->nph + 2) / 2)));
+  // the counter, done counts and error word start at zero (one launch per
+  // phase never writes them, and gofft_uneven_status reads the error word)
+  GF_CK(cudaMemset(u->d_ctr, 0, sizeof(unsigned long long) * (2 + (u->nph + 2) / 2)));
   GF_CK(cudaEventCreateWithFlags(&u->ev_fork, cudaEventDisableTiming));
   for (int k = 1; k < gofft_uneven::kLanes; k++) {
     GF_CK(cudaStreamCreateWithFlags(&u->lane[k], cudaStreamNonBlocking));
