@@ -49,6 +49,7 @@ struct gofft_uneven {
   std::vector<PhaseDesc> ph[2];        // forward, inverse (user pointers as tags)
   std::vector<int> ph_level;
   std::vector<int> ph_lane;            // per-phase launches: stream index (by class)
+  std::vector<int> launch_order;       // per-phase launches: phases in class order
   std::vector<std::shared_ptr<DevProg>> ph_prog;
   static constexpr int kLanes = 4;     // per-phase launches: classes spread over these streams
   cudaStream_t lane[kLanes] = {};      // lane[0] unused (the caller's stream)
@@ -63,7 +64,7 @@ struct gofft_uneven {
   size_t smem = 0;
   int grid = 0;
   long long spin_limit = 1ll << 24;
-  int extra_wait = 0;                  // test hook: a dependency that never completes
+  int extra_wait = 0;                  // test hook: dependencies that never complete
   const void *last_in[2] = {nullptr, nullptr};
   void *last_out[2] = {nullptr, nullptr};
   ~gofft_uneven() {
@@ -142,19 +143,26 @@ static int add_class(gofft_uneven *u, gofft_uneven::Cls &c, size_t *wsoff, std::
     return 0;
   }
   if (e.kind == K_FOURSTEP) {
-    char *w = carve((size_t)e.n * cnt * cs);
-    KArgs a1{};
-    a1.in = tag_side(&g_in_tag, c.d_ioff, 1, e.n2, e.n2);
-    a1.out = mk_side(w, e.n, 1, e.n2, e.n2);
-    a1.scale = 1.0;
-    a1.aux0 = e.tw4;
-    a1.ia = e.n;
-    const int p1 = push(OP_C2C_TW, e.p1, a1, cnt * e.n2, -1, 0, false);
-    KArgs a2{};
-    a2.in = mk_side(w, e.n, e.n2, 1, e.n1);
-    a2.out = tag_side(&g_out_tag, c.d_ooff, 1, e.n1, e.n1);
-    a2.scale = 1.0;
-    push(OP_C2C, e.p2, a2, cnt * e.n1, p1, 1, false);
+    // L2 blocks of signals (at most 48 MB of intermediate each), two phases
+    // per block: launched one launch per phase, a block's second pass reads
+    // its intermediate from L2
+    const long long kb = std::max<long long>(1, std::min<long long>(cnt, (48ll << 20) / (e.n * (long long)cs)));
+    for (long long b0 = 0; b0 < cnt; b0 += kb) {
+      const long long nb = std::min(kb, cnt - b0);
+      char *w = carve((size_t)e.n * nb * cs);
+      KArgs a1{};
+      a1.in = tag_side(&g_in_tag, c.d_ioff + b0, 1, e.n2, e.n2);
+      a1.out = mk_side(w, e.n, 1, e.n2, e.n2);
+      a1.scale = 1.0;
+      a1.aux0 = e.tw4;
+      a1.ia = e.n;
+      const int p1 = push(OP_C2C_TW, e.p1, a1, nb * e.n2, -1, 0, false);
+      KArgs a2{};
+      a2.in = mk_side(w, e.n, e.n2, 1, e.n1);
+      a2.out = tag_side(&g_out_tag, c.d_ooff + b0, 1, e.n1, e.n1);
+      a2.scale = 1.0;
+      push(OP_C2C, e.p2, a2, nb * e.n1, p1, 1, false);
+    }
     return 0;
   }
   if (e.kind == K_RADER && e.fused) {
@@ -277,9 +285,17 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
   std::vector<long long> raw_len;  // class length of each phase
   for (size_t r = 0; r < by_size.size(); r++) cls_lane[by_size[r]] = (int)(r % gofft_uneven::kLanes);
   for (size_t ci = 0; ci < u->cls.size(); ci++) {
+    const size_t first = raw.size();
     if (int rc = add_class(u.get(), u->cls[ci], &wsoff, raw, lvl, progs)) return rc;
-    raw_lane.resize(raw.size(), cls_lane[ci]);
     raw_len.resize(raw.size(), u->cls[ci].n);
+    if (u->cls[ci].ex->kind == K_FOURSTEP) {
+      // the class's L2 blocks (two phases each) rotate over the lanes, so one
+      // block's passes overlap the next block's
+      for (size_t r = first; r < raw.size(); r++)
+        raw_lane.push_back((int)((cls_lane[ci] + (r - first) / 2) % gofft_uneven::kLanes));
+    } else {
+      raw_lane.resize(raw.size(), cls_lane[ci]);
+    }
   }
   // order by level, keeping class order within a level; remap dependencies
   std::vector<int> order(raw.size());
@@ -287,6 +303,7 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return lvl[x] < lvl[y]; });
   std::vector<int> pos(raw.size());
   for (size_t i = 0; i < order.size(); i++) pos[order[i]] = (int)i;
+  u->launch_order = pos;  // per-phase launches keep class and block order
   u->nph = (int)raw.size();
   u->ph[0].resize(u->nph);
   long long first = 0;
@@ -384,8 +401,9 @@ static int patch(gofft_uneven *u, int dir, const void *in, void *out, cudaStream
     if (p.a.out.ptr == &g_in_tag) p.a.out.ptr = (void *)in;
   }
   if (u->extra_wait && u->nph > 1) {
-    // test hook: make the last phase wait on a phase that never completes
-    t[u->nph - 1].dep = 0;
+    // test hook: every phase after the first waits on the first, which
+    // never completes
+    for (int i = 1; i < u->nph; i++) t[i].dep = 0;
     t[0].ntiles += 1;
   }
   GF_CK(cudaStreamSynchronize(st));
@@ -416,7 +434,8 @@ extern "C" int gofft_uneven_exec(gofft_uneven *u, const void *in, void *out, int
   for (int k = 1; k < gofft_uneven::kLanes; k++) GF_CK(cudaStreamWaitEvent(u->lane[k], u->ev_fork, 0));
   std::vector<PhaseDesc> t = u->ph[dir];
   int rc = 0;
-  for (int i = 0; i < u->nph && !rc; i++) {
+  for (int r = 0; r < u->nph && !rc; r++) {
+    const int i = u->launch_order[r];
     PhaseDesc p = t[i];
     if (p.a.in.ptr == &g_in_tag) p.a.in.ptr = (void *)in;
     if (p.a.out.ptr == &g_out_tag) p.a.out.ptr = out;

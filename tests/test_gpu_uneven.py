@@ -137,9 +137,10 @@ def test_bounded_wait_reports_timeout():
 def test_timeout_drains_at_default_limit():
     # at the default poll limit, a dependency that never completes must cost
     # about one wait, not one wait per dependent tile: once a CTA gives up,
-    # the others stop waiting and the kernel drains.  The many-tile batch's
-    # last phase has several times more tiles than CTAs (each CTA would
-    # otherwise wait the full limit on every one of its tiles in turn).
+    # the others stop waiting and the kernel drains.  The hook makes every
+    # phase after the first wait; in the many-tile batch those phases hold
+    # several times more tiles than CTAs (each CTA would otherwise wait the
+    # full limit on every one of its tiles in turn).
     import time
     from fft_b200._lib import GOFFT_ETIMEOUT
     from fft_b200.device import UnevenBatch
@@ -148,7 +149,7 @@ def test_timeout_drains_at_default_limit():
         parts, flat = make_batch(lengths, 11, np.complex64)
         u = UnevenBatch("f32mixed", lengths)
         u.set(0, 1)   # the persistent launch
-        u.set(2, 1)   # hook: the last phase waits on work that never completes
+        u.set(2, 1)   # hook: the phases after the first wait on work that never completes
         d = u.describe()
         x = torch.from_numpy(flat).cuda()
         torch.cuda.synchronize()
@@ -161,7 +162,7 @@ def test_timeout_drains_at_default_limit():
         y = u(x)
         assert u.status() == 0
         check_all(lengths, y.cpu().numpy(), parts, "f32mixed")
-        return dt, d["phase_list"][-1]["tiles"], d["grid"]
+        return dt, sum(ph["tiles"] for ph in d["phase_list"][1:]), d["grid"]
 
     t_one, tiles_one, grid = timed([65536, 128])
     t_many, tiles_many, _ = timed([65536] * 160 + [128])
