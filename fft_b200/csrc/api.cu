@@ -212,7 +212,6 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
     }
   }
   if (int rc2 = plan_ws(p.get())) return rc2;
-  GF_CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   if (p->nlanes > 1) {
     GF_CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
     for (int i = 0; i + 1 < p->nlanes; i++) {
@@ -485,7 +484,16 @@ extern "C" int gofft_exec_c2r(gofft_plan *p, const void *in, int64_t nbins, void
 // ---------------------------------------------------------------------------
 // Host-pointer execution
 // ---------------------------------------------------------------------------
+// The plan's own stream for the host-pointer calls, created by the first
+// such call (under the plan's lock): plans used only on device pointers never
+// create one, which keeps plan construction short.
+static int ensure_stream(gofft_plan *p) {
+  if (!p->stream) GF_CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  return 0;
+}
+
 static int ensure_staging(gofft_plan *p, size_t in_b, size_t out_b) {
+  if (int rc = ensure_stream(p)) return rc;
   if (p->d_in_bytes < in_b) {
     if (p->d_in) cudaFree(p->d_in);
     p->d_in = nullptr;

@@ -6,12 +6,16 @@
     python -m fft_b200.prof fftn --shape 256,256,256 --prec f32mixed
     python -m fft_b200.prof rfft2 --prec f64 --wisdom wisdom.json
     python -m fft_b200.prof uneven-classes --prec f32mixed
+    python -m fft_b200.prof spectrogram --prec f32mixed --n 4194304
+    python -m fft_b200.prof filter2 --prec f32mixed --shape 512,512 --batch 32
 
 Prints the CUDA-event time per repetition (taken without a profiler; under a
 profiler the printed times are not measurements).  `roundtrip` is RFFT2 then
 IRFFT2 (the bench step).  `uneven-classes` times the length classes of the
 uneven batch (4096 complex64 signals, lengths drawn from seed 2 over
 {60, 128, 360, 1000, 1009, 4096, 10007, 65536}) one class at a time.
+`spectrogram` is the fused spectrogram of an --n-sample signal (Hann 2048,
+overlap 1536); `filter2` the 2-D spectral filter forward then backward.
 `--pipe off` turns the TMA-fed persistent line kernel off for comparison.
 """
 import argparse
@@ -57,7 +61,8 @@ def uneven_classes(prec, reps):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["rfft2", "irfft2", "roundtrip", "c2c", "fftn", "r2c", "uneven-classes"])
+    ap.add_argument("case", choices=["rfft2", "irfft2", "roundtrip", "c2c", "fftn", "r2c", "uneven-classes",
+                                     "spectrogram", "filter2"])
     ap.add_argument("--prec", default="f64")
     ap.add_argument("--n", type=int, default=1024)
     ap.add_argument("--shape", default="1024,1024")
@@ -88,7 +93,25 @@ def main():
     rdt = torch.float64 if a.prec == "f64" else torch.float32
     cdt = torch.complex128 if a.prec == "f64" else torch.complex64
     shape = [int(s) for s in a.shape.split(",")]
-    if a.case in ("rfft2", "irfft2", "r2c", "roundtrip"):
+    if a.case == "spectrogram":
+        from .device import spectrogram, window
+        sig = torch.from_numpy(g.standard_normal(a.n)).to(rdt).cuda()
+        win = window(0, 2048, a.prec)
+
+        def run():
+            spectrogram(sig, 2048, 1536, win, 1.0, a.prec)
+    elif a.case == "filter2":
+        from .function import SpectralFilter2
+        f = SpectralFilter2(a.prec, shape[0], shape[1], batch=a.batch)
+        xf = torch.from_numpy(g.random((a.batch, shape[0] * shape[1]))).to(rdt).cuda()
+        K = shape[1] // 2 + 1
+        Hf = torch.from_numpy(g.standard_normal(shape[0] * K) + 1j * g.standard_normal(shape[0] * K)).to(cdt).cuda()
+        yf = f.Forward(xf, Hf)
+
+        def run():
+            f.plan.filter2(xf, Hf, out=yf, saved=f.saved)
+            f.plan.vjp_filter2(yf, Hf, saved=f.saved, scratch=f.saved)
+    elif a.case in ("rfft2", "irfft2", "r2c", "roundtrip"):
         if a.case == "r2c":
             shape = [a.n]
         p = DevicePlan("r2c", a.prec, shape, batch=a.batch)
