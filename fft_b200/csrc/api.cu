@@ -203,7 +203,10 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       const long long budget = l2_block_bytes();
       const long long per = p->shape[0] * rc * (long long)csize(precision);
       const long long cmax = std::max<long long>(1, std::min<long long>(batch, budget / std::max<long long>(1, per)));
-      const long long nblocks = (batch + cmax - 1) / cmax;
+      // at least two blocks when there are two images, so the lanes overlap
+      // one block's row passes with the other block's column pass even when
+      // the whole batch would fit one L2 block
+      const long long nblocks = std::max<long long>((batch + cmax - 1) / cmax, batch >= 2 ? 2 : 1);
       // lanes: block i+1's passes overlap block i's (each pass alone ramps
       // up and drains; the other lanes fill those gaps)
       const bool lanes = nblocks > 1 && g_lanes.load() > 1;

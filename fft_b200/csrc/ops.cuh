@@ -121,7 +121,9 @@ struct OpC2CTwiddle {
     using TW = typename P::tw_t;
     uint32_t b, n2;
     a.out.lpb.divmod((uint32_t)line, b, n2);
-    const long long e = ((long long)n2 * i) % a.ia;
+    // n2 < N2 and i < N1, so n2 * i < N1 * N2 = N: the exponent needs no
+    // reduction modulo N
+    const uint32_t e = n2 * (uint32_t)i;
     return twmul(y, ld_keep(&((const TW *)a.aux0)[e]));
   }
   template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
@@ -813,7 +815,7 @@ struct OpRaderFS1 {  // aux0 perm, aux1 W_cl table, aux2 x0s; ia = cl, ib = q
     tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
       uint32_t b, n2;
       a.out.lpb.divmod((uint32_t)(line0 + l), b, n2);
-      const long long e = ((long long)n2 * i) % a.ia;
+      const uint32_t e = n2 * (uint32_t)i;  // n2 < N2, i < N1: below cl, no reduction
       out[off] = twmul(line_view<C>(a, l, sb)[i], __ldg(&((const TW *)a.aux1)[e]));
     });
   }

@@ -96,7 +96,7 @@ def main():
     if a.case == "spectrogram":
         from .device import spectrogram, window
         sig = torch.from_numpy(g.standard_normal(a.n)).to(rdt).cuda()
-        win = window(0, 2048, a.prec)
+        win = window("hann", 2048, a.prec)
 
         def run():
             spectrogram(sig, 2048, 1536, win, 1.0, a.prec)

@@ -64,7 +64,9 @@ def test_pipe_rfft2_1024(prec, variant, schedule):
     from fft_b200.device import DevicePlan
     from fft_b200._lib import GOFFT_F64, GOFFT_F32MIXED
     schedule(GOFFT_F64 if prec == "f64" else GOFFT_F32MIXED, 512, variant)
-    B = 3 if prec == "f64" else 8
+    # every L2 block (two per plan at least) needs two tiles per SM for the
+    # pipelined kernel: 6 FP64 images make blocks of 3, 8 FP32 images of 4
+    B = 6 if prec == "f64" else 8
     rdt = torch.float64 if prec == "f64" else torch.float32
     x = rng(31).standard_normal((B, 1024 * 1024))
     xt = torch.from_numpy(x).to(rdt).cuda()
@@ -84,7 +86,7 @@ def test_pipe_row_tail(prec):
     """1001 rows per image: the last row tile is partial (FP32: its bins are
     not a multiple of 16 bytes, so that tile falls back to element copies)."""
     from fft_b200.device import DevicePlan
-    B, R, C = 3, 1001, 1024
+    B, R, C = 6, 1001, 1024
     rdt = torch.float64 if prec == "f64" else torch.float32
     x = rng(32).standard_normal((B, R * C))
     xt = torch.from_numpy(x).to(rdt).cuda()
@@ -123,7 +125,7 @@ def test_pipe_complex_rows_and_columns():
 def test_pipe_adjoints():
     """The real adjoints run the packed rows with the edge-bin weights."""
     from fft_b200.device import DevicePlan
-    B = 3
+    B = 6
     g = rng(34)
     p = DevicePlan("r2c", "f64", [1024, 1024], batch=B)
     G = torch.from_numpy(g.standard_normal((B, 1024 * 513)) + 1j * g.standard_normal((B, 1024 * 513))).cuda()
