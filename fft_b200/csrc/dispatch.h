@@ -66,6 +66,7 @@ struct EwArgs {
   cudaError_t scatter(const Side &dst, const void *src, const EwArgs &e, cudaStream_t st);    \
   cudaError_t stage_tw(void *tw, const StageTab &t, long long total, cudaStream_t st);        \
   cudaError_t roots(void *tw, long long L, long long count, cudaStream_t st);                 \
+  cudaError_t roots_step(void *tw, long long L, long long count, long long step, cudaStream_t st); \
   cudaError_t spectrum(void *dst, const double2 *src, double s, long long n, cudaStream_t st); \
   cudaError_t untangle(const Side &dst, const void *Z, long long nl, int m, const void *tw,   \
                        double wsc, cudaStream_t st);                                          \

@@ -204,7 +204,11 @@ static inline int ew_blocks(long long total) {
     return cudaGetLastError();                                                                 \
   }                                                                                            \
   cudaError_t roots(void *tw, long long L, long long count, cudaStream_t st) {                 \
-    k_gen_roots<TW><<<ew_blocks(count), 256, 0, st>>>((TW *)tw, L, count);                    \
+    k_gen_roots<TW><<<ew_blocks(count), 256, 0, st>>>((TW *)tw, L, count, 1);                 \
+    return cudaGetLastError();                                                                 \
+  }                                                                                            \
+  cudaError_t roots_step(void *tw, long long L, long long count, long long step, cudaStream_t st) { \
+    k_gen_roots<TW><<<ew_blocks(count), 256, 0, st>>>((TW *)tw, L, count, step);              \
     return cudaGetLastError();                                                                 \
   }                                                                                            \
   cudaError_t spectrum(void *dst, const double2 *src, double s, long long n, cudaStream_t st) { \

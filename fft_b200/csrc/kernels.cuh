@@ -383,11 +383,11 @@ __global__ void k_gen_stage_tw(TW *tw, StageTab st, long long total) {
   }
 }
 
-// W_L^k for k = 0..count-1 (four-step and real-untangle tables).
-template <class TW> __global__ void k_gen_roots(TW *tw, long long L, long long count) {
+// W_L^(k step) for k = 0..count-1 (four-step and real-untangle tables).
+template <class TW> __global__ void k_gen_roots(TW *tw, long long L, long long count, long long step) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < count;
        k += (long long)gridDim.x * blockDim.x)
-    put_tw(tw, k, root_of_unity(k, L));
+    put_tw(tw, k, root_of_unity(k * step, L));
 }
 
 // Scale an FP64 spectrum by s and store it in the precision's spectrum form.

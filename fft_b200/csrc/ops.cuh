@@ -109,8 +109,19 @@ struct OpC2C {
   }
 };
 
+// y * W_N^e from a split table (see OpC2CTwiddle): W_N^(e mod 2^sh), then
+// W_N^(2^sh floor(e / 2^sh)).
+template <class P>
+GF_DEV Cx<P> split_tw(Cx<P> y, const typename P::tw_t *t, uint32_t e, int sh) {
+  const uint32_t S = 1u << sh;
+  return twmul(twmul(y, ld_keep(&t[e & (S - 1)])), ld_keep(&t[S + (e >> sh)]));
+}
+
 // Four-step pass 1: element k1 of line n2 (the line's index within its batch)
-// is multiplied by W_N^{n2*k1} from the table aux0 (N = ia entries).
+// is multiplied by W_N^e, e = n2*k1 < N, as W_N^(e mod S) * W_N^(S floor(e/S))
+// from the split table aux0 (S = 2^ic entries, then ceil(N/S) entries):
+// two small tables that stay in L1 instead of one of N entries read at
+// scattered places.  ia = N.
 struct OpC2CTwiddle {
   static constexpr bool kConv = false, kFG = true, kTG = true;
   static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
@@ -123,8 +134,7 @@ struct OpC2CTwiddle {
     a.out.lpb.divmod((uint32_t)line, b, n2);
     // n2 < N2 and i < N1, so n2 * i < N1 * N2 = N: the exponent needs no
     // reduction modulo N
-    const uint32_t e = n2 * (uint32_t)i;
-    return twmul(y, ld_keep(&((const TW *)a.aux0)[e]));
+    return split_tw<P>(y, (const TW *)a.aux0, n2 * (uint32_t)i, a.ic);
   }
   template <class P> static GF_DEV void gstore(const KArgs &a, const LineCtx &c, int i, Cx<P> y) {
     if (!c.valid) return;
@@ -775,7 +785,7 @@ struct OpSpectro {
 // Signals of the phase are batches b; lines within a signal are the
 // sides' lpb groups.
 // ---------------------------------------------------------------------------
-struct OpRaderFS1 {  // aux0 perm, aux1 W_cl table, aux2 x0s; ia = cl, ib = q
+struct OpRaderFS1 {  // aux0 perm, aux1 split W_cl table (2^ic + ...), aux2 x0s; ia = cl, ib = q
   static constexpr bool kConv = false, kFG = false, kTG = false;
   static GF_DEV bool first_conj(const KArgs &a) { return a.cj_in; }
   template <class P> static GF_DEV Cx<P> gload(const KArgs &, const LineCtx &, int) { return Cx<P>(); }
@@ -815,8 +825,8 @@ struct OpRaderFS1 {  // aux0 perm, aux1 W_cl table, aux2 x0s; ia = cl, ib = q
     tile_loop(a.out, a.lpc, a.lp.n, a.ndiv, a.lpcdiv, line0, a.nlines, [&](int l, int i, long long off) {
       uint32_t b, n2;
       a.out.lpb.divmod((uint32_t)(line0 + l), b, n2);
-      const uint32_t e = n2 * (uint32_t)i;  // n2 < N2, i < N1: below cl, no reduction
-      out[off] = twmul(line_view<C>(a, l, sb)[i], __ldg(&((const TW *)a.aux1)[e]));
+      // n2 < N2, i < N1: the exponent is below cl, no reduction
+      out[off] = split_tw<P>(line_view<C>(a, l, sb)[i], (const TW *)a.aux1, n2 * (uint32_t)i, a.ic);
     });
   }
 };

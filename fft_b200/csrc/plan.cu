@@ -940,6 +940,7 @@ int Exec1D::exec(const Side &in, const Side &out, long long nl, int cji, int cjo
       a1.scale = 1.0;
       a1.aux0 = tw4;
       a1.ia = n;
+      a1.ic = tw4_sh;
       if (int rc = launch_line(OP_C2C_TW, *p1, a1, nl * n2, st)) return rc;
       // pass 2: n1 rows of length n2, written transposed
       KArgs a2{};
@@ -1102,6 +1103,7 @@ void Exec1D::rader_phases(const Side &in, long long Din, const Side &out, long l
   f1.a.scale = 1.0;
   f1.a.aux0 = perm;
   f1.a.aux1 = cv.tw4;
+  f1.a.ic = cv.tw4_sh;
   f1.a.aux2 = x0s;
   f1.a.ia = cl;
   f1.a.ib = q;
@@ -1123,6 +1125,7 @@ void Exec1D::rader_phases(const Side &in, long long Din, const Side &out, long l
   f3.a.out = mk_side(W1, cl, 1, N2, N2);
   f3.a.scale = 1.0;
   f3.a.aux0 = cv.tw4;
+  f3.a.ic = cv.tw4_sh;
   f3.a.ia = cl;
   RaderPhase f4{};
   f4.op = OP_RADER_FS4;
@@ -1274,8 +1277,15 @@ static int build_exec(long long n, int prec, std::shared_ptr<Exec1D> &out) {
     ex->p1 = get_prog(ex->n1, prec);
     ex->p2 = get_prog(ex->n2, prec);
     if (!ex->p1 || !ex->p2) return 3;
-    GF_CK(cudaMalloc(&ex->tw4, n * twsize(prec)));
-    GF_CK(GF_PREC_CALL(prec, roots, ex->tw4, n, n, 0));
+    // split twiddle table: S = 2^sh >= sqrt(n) entries W_n^e, then
+    // ceil(n / S) entries W_n^(S j)
+    int sh = 0;
+    while ((1ll << (2 * sh)) < n) sh++;
+    const long long S = 1ll << sh, J = (n + S - 1) / S;
+    ex->tw4_sh = sh;
+    GF_CK(cudaMalloc(&ex->tw4, (S + J) * twsize(prec)));
+    GF_CK(GF_PREC_CALL(prec, roots, ex->tw4, n, S, 0));
+    GF_CK(GF_PREC_CALL(prec, roots_step, (char *)ex->tw4 + S * twsize(prec), n, J, S, 0));
     GF_CK(cudaStreamSynchronize(0));
     out = ex;
     return 0;

@@ -89,7 +89,8 @@ struct Exec1D {
   std::shared_ptr<DevProg> p1, p2;      // FOURSTEP: lengths n1, n2
   std::shared_ptr<const Exec1D> sub;    // multi-pass convolution at cl / m
   long long n1 = 0, n2 = 0;
-  void *tw4 = nullptr;                  // FOURSTEP: W_n^e, e < n
+  void *tw4 = nullptr;                  // FOURSTEP: W_n^e for e < 2^tw4_sh, then W_n^(2^tw4_sh j)
+  int tw4_sh = 0;                       //   (the split twiddle table of OpC2CTwiddle)
   bool fused = false;
   // Rader whose convolution fits one CTA's shared memory but not the
   // register-staged line kernels: the in-place kernel (rader_ip.cuh), with

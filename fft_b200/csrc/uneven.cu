@@ -156,6 +156,7 @@ static int add_class(gofft_uneven *u, gofft_uneven::Cls &c, size_t *wsoff, std::
       a1.scale = 1.0;
       a1.aux0 = e.tw4;
       a1.ia = e.n;
+      a1.ic = e.tw4_sh;
       const int p1 = push(OP_C2C_TW, e.p1, a1, nb * e.n2, -1, 0, false);
       KArgs a2{};
       a2.in = mk_side(w, e.n, e.n2, 1, e.n1);
