@@ -355,8 +355,11 @@ extern "C" int gofft_uneven_create(int precision, const int64_t *lengths, int64_
     const bool conv = p.op == OP_RADER || p.op == OP_BLUE;
     // an in-shared-memory Rader item runs on every thread of the CTA
     u->block = std::max(u->block, p.op == OP_RADER_IP ? 512 : p.a.lpc * p.a.lp.T);
-    u->smem = std::max(u->smem, (size_t)p.a.lpc * spad_size(p.a.lp.n) * csize(precision) +
-                                    (conv ? 2 * p.a.lpc * csize(precision) : 0));
+    if (p.op == OP_RADER_IP)  // the unpadded convolution (rader_ip.cuh)
+      u->smem = std::max(u->smem, (size_t)p.a.lp.n * csize(precision));
+    else
+      u->smem = std::max(u->smem, (size_t)p.a.lpc * spad_size(p.a.lp.n) * csize(precision) +
+                                      (conv ? 2 * p.a.lpc * csize(precision) : 0));
   }
   u->block = (u->block + 31) / 32 * 32;
   const void *kp = persist_fn(precision);

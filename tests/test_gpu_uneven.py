@@ -52,6 +52,22 @@ def test_uneven_c3_lengths(prec, persistent):
     assert d["persistent"] == persistent
 
 
+@pytest.mark.parametrize("persistent", [1, 0])
+def test_uneven_longest_inplace_rader_f64(persistent):
+    """13721 in FP64: its cyclic convolution of 13720 complex128 (219 KB) is
+    the longest that runs in one CTA's shared memory; the persistent launch
+    is sized for the unpadded convolution and still fits an SM."""
+    from fft_b200.device import DevicePlan, UnevenBatch
+    assert DevicePlan("c2c", "f64", [13721]).describe()["axes"][0]["inplace"] == 1
+    lengths = [13721, 64, 13721, 1000, 13721]
+    parts, flat = make_batch(lengths, 9, np.complex128)
+    u = UnevenBatch("f64", lengths)
+    u.set(0, persistent)
+    y = u(torch.from_numpy(flat).cuda())
+    assert u.status() == 0
+    check_all(lengths, y.cpu().numpy(), parts, "f64")
+
+
 def test_uneven_inplace_and_offsets():
     from fft_b200.device import UnevenBatch
     lengths = [1009, 60, 65536, 17, 641, 10007, 128]
