@@ -96,6 +96,10 @@ cudaError_t gen_blue_kernel(double2 *b, const double2 *w, long long n, long long
 const void *rader_ip_kernel_f64(int *threads);
 const void *rader_ip_kernel_f32(int *threads);
 const void *rader_ip_kernel_f32c(int *threads);
+// the two-CTA (cluster) form of the same transform
+const void *rader_ip2_kernel_f64(int *threads);
+const void *rader_ip2_kernel_f32(int *threads);
+const void *rader_ip2_kernel_f32c(int *threads);
 // The persistent multi-phase kernel (k_persist) of each precision.
 const void *persist_kernel_f64();
 const void *persist_kernel_f32();

@@ -5,4 +5,8 @@ const void *rader_ip_kernel_f32c(int *threads) {
   *threads = rip_threads<PrecF32C>();
   return (const void *)k_rader_ip<PrecF32C>;
 }
+const void *rader_ip2_kernel_f32c(int *threads) {
+  *threads = rip_threads<PrecF32C>();
+  return (const void *)k_rader_ip2<PrecF32C>;
+}
 }  // namespace gf

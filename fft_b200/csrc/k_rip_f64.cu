@@ -5,4 +5,8 @@ const void *rader_ip_kernel_f64(int *threads) {
   *threads = rip_threads<PrecF64>();
   return (const void *)k_rader_ip<PrecF64>;
 }
+const void *rader_ip2_kernel_f64(int *threads) {
+  *threads = rip_threads<PrecF64>();
+  return (const void *)k_rader_ip2<PrecF64>;
+}
 }  // namespace gf

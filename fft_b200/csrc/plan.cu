@@ -758,9 +758,63 @@ static int try_pipe(int op, const DevProg &dp, KArgs a, long long nlines, cudaSt
   return 1;
 }
 
+// Two-CTA form: clusters of two CTAs, each holding half the convolution
+// (persistent over the signals, one cluster per pair of SMs at most).
+static int launch_rader_ip2(const DevProg &dp, KArgs a, long long nlines, cudaStream_t st) {
+  int threads = 0;
+  const void *f = dp.prec == F64 ? rader_ip2_kernel_f64(&threads)
+                                 : (dp.prec == F32 ? rader_ip2_kernel_f32(&threads) : rader_ip2_kernel_f32c(&threads));
+  a.lp = dp.lp;
+  a.nlines = nlines;
+  a.lpc = 1;
+  a.ndiv = FastDiv((uint32_t)dp.n);
+  a.lpcdiv = FastDiv(1);
+  a.flags = 0;
+  const size_t smem = (size_t)(dp.n / 2) * csize(dp.prec);
+  if (int rc = ensure_smem((KFn)f, smem)) return rc;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3((unsigned)threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3((unsigned)(2 * std::min<long long>(nlines, num_sms() / 2)));
+  int clusters = 0;
+  GF_CK(cudaOccupancyMaxActiveClusters(&clusters, f, &cfg));
+  if (clusters < 1) return set_err(5, "two-CTA Rader kernel does not fit a pair of SMs");
+  cfg.gridDim = dim3((unsigned)(2 * std::min<long long>(nlines, clusters)));
+  count_launch();
+  TimingRec rec;
+  const bool timed = g_timing.load() != 0;
+  if (timed) {
+    cudaEventCreate(&rec.a);
+    cudaEventCreate(&rec.b);
+    cudaEventRecord(rec.a, st);
+  }
+  void *args[] = {&a};
+  GF_CK(cudaLaunchKernelExC(&cfg, f, args));
+  if (timed) {
+    cudaEventRecord(rec.b, st);
+    std::ostringstream k;
+    k << op_name(OP_RADER_IP) << "/p=" << a.ia << "/cl=" << dp.n << "/prec=" << dp.prec << "/T=" << threads
+      << "/ctas=2";
+    rec.key = k.str();
+    rec.bytes = algo_bytes(OP_RADER_IP, dp, a, nlines);
+    std::lock_guard<std::mutex> lk(g_tmu);
+    g_trecs.push_back(rec);
+  }
+  return 0;
+}
+
 // The in-shared-memory Rader kernel: one CTA per signal (persistent over the
 // signals), the convolution of length dp.n in dynamic shared memory.
 static int launch_rader_ip(const DevProg &dp, KArgs a, long long nlines, cudaStream_t st) {
+  if (dp.ctas == 2) return launch_rader_ip2(dp, a, nlines, st);
   int threads = 0;
   const void *f = dp.prec == F64 ? rader_ip_kernel_f64(&threads)
                                  : (dp.prec == F32 ? rader_ip_kernel_f32(&threads) : rader_ip_kernel_f32c(&threads));
@@ -789,7 +843,8 @@ static int launch_rader_ip(const DevProg &dp, KArgs a, long long nlines, cudaStr
   if (timed) {
     cudaEventRecord(rec.b, st);
     std::ostringstream k;
-    k << op_name(OP_RADER_IP) << "/p=" << a.ia << "/cl=" << dp.n << "/prec=" << dp.prec << "/T=" << threads;
+    k << op_name(OP_RADER_IP) << "/p=" << a.ia << "/cl=" << dp.n << "/prec=" << dp.prec << "/T=" << threads
+      << "/ctas=1";
     rec.key = k.str();
     rec.bytes = algo_bytes(OP_RADER_IP, dp, a, nlines);
     std::lock_guard<std::mutex> lk(g_tmu);
@@ -1158,7 +1213,7 @@ std::string Exec1D::describe() const {
   if (kind == K_FOURSTEP) o << ",\"n1\":" << n1 << ",\"n2\":" << n2 << ",\"p1\":" << sched(*p1) << ",\"p2\":" << sched(*p2);
   if (kind == K_RADER)
     o << ",\"g\":" << g << ",\"cl\":" << cl << ",\"cyclic\":" << cyclic << ",\"fused\":" << (fused ? 1 : 0)
-      << ",\"inplace\":" << (inplace ? 1 : 0);
+      << ",\"inplace\":" << (inplace ? 1 : 0) << ",\"inplace_ctas\":" << (inplace ? ipprog->ctas : 0);
   if (kind == K_BLUE) o << ",\"m\":" << m << ",\"fused\":" << (fused ? 1 : 0);
   if ((kind == K_RADER || kind == K_BLUE) && fused && prog) o << ",\"prog\":" << sched(*prog);
   if ((kind == K_RADER || kind == K_BLUE) && !fused && sub) o << ",\"conv\":" << sub->describe();
@@ -1194,16 +1249,26 @@ static int make_spectrum(int prec, double2 *b, long long L, void **spec_out) {
 // planes W_{R S}^{j m} (j < S, the Stockham table layout with ns = S), and
 // the kernel spectrum permuted to the digit-reversed order the forward stages
 // leave: A[k] at pos = sum_s m_s S_s for k = m_0 + R_0 m_1 + R_0 R_1 m_2 + ...
+// A convolution too long for one CTA but even, whose first (power-of-two)
+// radix is 2, 4 or 8 and whose half fits, runs on a cluster of two CTAs
+// (k_rader_ip2), each holding half the line.
 // Returns 0 when built, 1 when the length does not qualify, else an error.
 static int build_rader_ip(Exec1D &ex) {
   const long long cl = ex.cl;
   const int prec = ex.prec;
-  if ((size_t)cl * csize(prec) > max_smem_optin()) return 1;
   const std::vector<int> rad = gpu_radices(cl, 3);
   if (rad.empty() || (int)rad.size() > GF_MAXST) return 1;
   for (int R : rad)
     if (!rip_radix_ok(R)) return 1;
+  // the kernels' static shared memory (two values) sits beside the line
+  const size_t room = max_smem_optin() - 256;
+  int ctas = 1;
+  if ((size_t)cl * csize(prec) > room) {
+    if (cl % 2 || !rip2_first_radix_ok(rad[0]) || (size_t)(cl / 2) * csize(prec) > room) return 1;
+    ctas = 2;
+  }
   auto dp = std::make_shared<DevProg>();
+  dp->ctas = ctas;
   dp->n = (int)cl;
   dp->prec = prec;
   dp->device = cur_device();

@@ -65,6 +65,7 @@ int get_uneven_mode(int prec);
 
 struct DevProg {
   int n = 0, prec = 0, maxe = 16, device = 0;
+  int ctas = 1;  // in-shared-memory Rader: CTAs (a cluster) per signal
   LineProg lp{};
   void *tw = nullptr;
   void *tw_hi = nullptr;  // FP32-mixed: hi parts as FP32 pairs

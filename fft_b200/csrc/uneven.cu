@@ -190,7 +190,9 @@ static int add_class(gofft_uneven *u, gofft_uneven::Cls &c, size_t *wsoff, std::
     push(OP_BLUE, e.prog, a, cnt, -1, 0, true);
     return 0;
   }
-  if (e.kind == K_RADER && e.inplace) {
+  // (the two-CTA form is not a persistent-kernel phase: those classes take
+  // the four passes below)
+  if (e.kind == K_RADER && e.inplace && e.ipprog->ctas == 1) {
     KArgs a{};
     a.in = in1;
     a.out = out1;
