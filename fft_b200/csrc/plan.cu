@@ -787,7 +787,9 @@ static int launch_rader_ip2(const DevProg &dp, KArgs a, long long nlines, cudaSt
   int clusters = 0;
   GF_CK(cudaOccupancyMaxActiveClusters(&clusters, f, &cfg));
   if (clusters < 1) return set_err(5, "two-CTA Rader kernel does not fit a pair of SMs");
-  cfg.gridDim = dim3((unsigned)(2 * std::min<long long>(nlines, clusters)));
+  const long long full = std::min<long long>(nlines, clusters);
+  const long long rounds = (nlines + full - 1) / full;
+  cfg.gridDim = dim3((unsigned)(2 * ((nlines + rounds - 1) / rounds)));
   count_launch();
   TimingRec rec;
   const bool timed = g_timing.load() != 0;
@@ -829,7 +831,11 @@ static int launch_rader_ip(const DevProg &dp, KArgs a, long long nlines, cudaStr
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, threads, smem);
   if (per_sm < 1) return set_err(5, "in-place Rader kernel does not fit an SM");
-  const long long grid = std::min<long long>(nlines, (long long)per_sm * num_sms());
+  // as many rounds of signals as the full grid needs, over as few CTAs as
+  // give that many rounds (the rest of the SMs stay free for concurrent work)
+  const long long full = std::min<long long>(nlines, (long long)per_sm * num_sms());
+  const long long rounds = (nlines + full - 1) / full;
+  const long long grid = (nlines + rounds - 1) / rounds;
   count_launch();
   TimingRec rec;
   const bool timed = g_timing.load() != 0;
