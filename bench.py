@@ -344,6 +344,70 @@ def _rel(got, want):
     return float(np.linalg.norm(got - want) / np.linalg.norm(want))
 
 
+# The reference's published single-signal timings (BENCHMARKS.md:26-45, :88,
+# :121-123; Apple M4 Max, Go 1.26.4, FP64, one signal per call, one core for
+# 1-D, 16 cores for FFT2), ns per transform.
+PUBLISHED = [("c2c", [256], 716), ("c2c", [1024], 3395), ("c2c", [4096], 16383), ("c2c", [65536], 377784),
+             ("c2c", [1048576], 13355742), ("c2c", [1000], 5850), ("c2c", [1009], 17214),
+             ("c2c", [10007], 369217), ("r2c", [1024], 2289), ("r2c", [4096], 10320), ("r2c", [65536], 230167),
+             ("c2r", [1024], 3517), ("c2c", [256, 256], 208437), ("c2c", [512, 512], 633920),
+             ("c2c", [1024, 1024], 2784623)]
+
+
+def published_rows(peak):
+    """Each transform the reference publishes a timing for, in FP64 on the
+    B200: a batch of signals whose input exceeds L2 (>= 256 MB), timed with
+    CUDA events (mean of 5 after 3 warm-ups), beside the reference's published
+    ns per transform (one signal per call on the CPU; a different machine and
+    a different unit of work: a per-transform throughput, not a latency), and
+    the relative L2 error of one signal against the oracle."""
+    import torch
+    from oracle import oracle as O
+    from fft_b200.device import DevicePlan
+    rows = {}
+    g = np.random.default_rng(11)
+    for kind, shape, ref_ns in PUBLISHED:
+        n = int(np.prod(shape))
+        real = kind != "c2c"
+        nb = n // 2 + 1 if real else n
+        in_b = n * 8 if kind == "r2c" else (nb * 16 if kind == "c2r" else n * 16)
+        out_b = nb * 16 if kind == "r2c" else (n * 8 if kind == "c2r" else n * 16)
+        B = int(min(65536, max(1, (256 << 20) // in_b)))
+        p = DevicePlan("r2c" if real else "c2c", "f64", shape, batch=B)
+        if kind == "r2c":
+            x = torch.from_numpy(g.standard_normal((B, n))).cuda()
+            y = torch.empty((B, nb), dtype=torch.complex128, device="cuda")
+            fn = lambda: p.r2c(x, out=y)
+        elif kind == "c2r":
+            src = g.standard_normal((B, n))
+            x = torch.from_numpy(np.fft.rfft(src, axis=1)).cuda()
+            y = torch.empty((B, n), dtype=torch.float64, device="cuda")
+            fn = lambda: p.c2r(x, out=y)
+        else:
+            x = torch.from_numpy(g.standard_normal((B, n)) + 1j * g.standard_normal((B, n))).cuda()
+            y = torch.empty_like(x)
+            fn = lambda: p.c2c(x, out=y)
+        ms = _events_ms(torch, fn, 5)
+        fn()
+        torch.cuda.synchronize()
+        x0 = x[B - 1].cpu().numpy()
+        if kind == "r2c":
+            want = O.rfft(x0)
+        elif kind == "c2r":
+            want = O.irfft(x0, n)
+        else:
+            want = O.fft(x0) if len(shape) == 1 else O.fftn(x0, shape)
+        ns = ms * 1e6 / B
+        gbs = B * (in_b + out_b) / (ms / 1e3) / 1e9
+        key = "%s %s" % ("fft2" if len(shape) == 2 else kind, "x".join(str(s) for s in shape))
+        rows[key] = {"batch": B, "ns_per_transform": round(ns, 2), "transforms_per_s": round(1e9 / ns, 1),
+                     "gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 4),
+                     "reference_ns_per_op_m4max": ref_ns, "per_transform_ratio": round(ref_ns / ns, 1),
+                     "rel_l2_vs_oracle": _rel(y[B - 1].cpu().numpy(), want)}
+        del x, y, p
+    return rows
+
+
 def extra_workloads(peak):
     """The other configurations of the transform path, each timed on the
     device with CUDA events and checked against the oracle on a sample:
@@ -623,6 +687,7 @@ def run_ours(args):
     if rank != 0:
         return 0
     extra = extra_workloads(peak) if (world == 1 and not args.no_extra) else None
+    published = published_rows(peak) if (world == 1 and not args.no_extra) else None
     cpu = cpu_baseline() if world == 1 else None
     clocks = clk.summary()
     line = {
@@ -657,7 +722,7 @@ def run_ours(args):
                                            "other lane's overlapping work"}},
         "plan_construction": pcost,
         "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu,
-        "other_workloads": extra,
+        "other_workloads": extra, "published_rows": published,
     }
     if world > 1:
         import torch.distributed as dist

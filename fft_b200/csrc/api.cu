@@ -30,6 +30,7 @@ struct gofft_plan {
   size_t lane_bytes = 0;                          // workspace per lane
   size_t lane_buf = 0;                            // block buffer at the start of a lane region
   long long nplane_blocks = 0;                    // complex N-D: planes per L2 block (0: unblocked)
+  long long line_blocks = 0;                      // 1-D complex four-step: signals per L2 block (0: unblocked)
   cudaStream_t lane[2] = {nullptr, nullptr};      // the second lane's stream (lane[1] unused)
   cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
   size_t ws_bytes = 0;
@@ -104,7 +105,12 @@ static long long extent(long long batch, long long dist, long long len, long lon
 
 static int plan_ws(gofft_plan *p) {
   size_t need = 0;
-  if (p->kind == GOFFT_C2C) {
+  if (p->kind == GOFFT_C2C && p->line_blocks > 0) {
+    // one region per lane, each for one block of signals
+    p->lane_buf = 0;
+    p->lane_bytes = (p->ax[0]->ws_bytes(p->line_blocks) + 255) & ~(size_t)255;
+    need = (size_t)p->nlanes * p->lane_bytes;
+  } else if (p->kind == GOFFT_C2C) {
     for (int a = 0; a < p->rank; a++) {
       const long long lines = (p->rank == 1 ? p->batch : p->batch * (p->total / p->shape[a]));
       need = std::max(need, p->ax[a]->ws_bytes(lines));
@@ -174,6 +180,18 @@ extern "C" int gofft_plan_create(int kind, int precision, const int64_t *shape, 
       auto ex = get_exec(p->shape[a], precision);
       if (!ex) return GOFFT_ECUDA;
       p->ax.push_back(ex);
+    }
+    if (rank == 1 && p->ax[0]->kind == K_FOURSTEP) {
+      // four-step signals per L2 block: a block's pass-1 output stays in L2
+      // for pass 2; blocks alternate lanes, so one block's passes overlap
+      // the next block's
+      const long long per = p->shape[0] * (long long)csize(precision);
+      const long long cmax = std::max<long long>(1, std::min<long long>(batch, l2_block_bytes() / per));
+      const long long nblocks = (batch + cmax - 1) / cmax;
+      if (nblocks > 1 && g_lanes.load() > 1) {
+        p->nlanes = g_lanes.load();
+        p->line_blocks = lane_chunk(batch, nblocks, p->nlanes);
+      }
     }
     if (rank >= 2 && p->shape[rank - 1] > 1 && p->shape[rank - 2] > 1) {
       // planes (the last two axes) per L2 block: both axes run while a
@@ -245,7 +263,8 @@ extern "C" int64_t gofft_plan_describe(const gofft_plan *p, char *buf, int64_t c
   o << "{\"kind\":\"" << (p->kind == GOFFT_C2C ? "c2c" : "r2c") << "\",\"precision\":" << p->prec
     << ",\"batch\":" << p->batch << ",\"shape\":[";
   for (int a = 0; a < p->rank; a++) o << (a ? "," : "") << p->shape[a];
-  o << "],\"workspace\":" << p->ws_bytes << ",\"chunk\":" << p->chunk << ",\"axes\":[";
+  o << "],\"workspace\":" << p->ws_bytes << ",\"chunk\":" << p->chunk << ",\"line_blocks\":" << p->line_blocks
+    << ",\"axes\":[";
   for (size_t a = 0; a < p->ax.size(); a++) o << (a ? "," : "") << p->ax[a]->describe();
   o << "]";
   if (p->rx) o << ",\"real\":" << p->rx->describe();
@@ -332,6 +351,21 @@ struct Lanes {
 // the inverse's 1/n per axis.  The plain transforms have cj == scaled; the
 // adjoints flip the direction and keep the scaling.
 static int exec_c2c_dir(gofft_plan *p, const void *in, void *out, int cj, int scaled, cudaStream_t st) {
+  if (p->rank == 1 && p->line_blocks > 0) {
+    const double sc = scaled ? 1.0 / (double)p->shape[0] : 1.0;
+    const size_t c = csize(p->prec);
+    const long long kb0 = p->line_blocks;
+    Lanes ln(p, st);
+    if (int e = ln.fork((p->batch + kb0 - 1) / kb0)) return e;
+    long long blk = 0;
+    for (long long b0 = 0; b0 < p->batch; b0 += kb0, blk++) {
+      const long long kb = std::min(kb0, p->batch - b0);
+      const Side si = mk_side((char *)in + (size_t)b0 * p->idist * c, p->idist, 0, p->istride, 1);
+      const Side so = mk_side((char *)out + (size_t)b0 * p->odist * c, p->odist, 0, p->ostride, 1);
+      if (int e = p->ax[0]->exec(si, so, kb, cj, cj, sc, ln.sub(blk), ln.stream(blk))) return ln.join(e);
+    }
+    return ln.join(GOFFT_OK);
+  }
   if (p->rank == 1) {
     const double sc = scaled ? 1.0 / (double)p->shape[0] : 1.0;
     return p->ax[0]->exec(mk_side((void *)in, p->idist, 0, p->istride, 1),
