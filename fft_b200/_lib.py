@@ -85,6 +85,7 @@ SIGNATURES = {
     "gofft_set_l2_block_bytes": (ctypes.c_int, [_i64]),
     "gofft_set_lanes": (ctypes.c_int, [ctypes.c_int]),
     "gofft_set_tma_pipeline": (ctypes.c_int, [ctypes.c_int]),
+    "gofft_set_dependent_launch": (ctypes.c_int, [ctypes.c_int]),
     "gofft_pipeline_status": (ctypes.c_int, []),
     "gofft_set_schedule": (ctypes.c_int, [ctypes.c_int, _i64, ctypes.c_int]),
     "gofft_hamming": (ctypes.c_int, [_i64, _vp]),

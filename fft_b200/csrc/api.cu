@@ -1170,6 +1170,11 @@ extern "C" int gofft_set_tma_pipeline(int on) {
   return GOFFT_OK;
 }
 extern "C" int gofft_pipeline_status(void) { return pipe_status(true); }
+extern "C" int gofft_set_dependent_launch(int mode) {
+  if (mode < 0 || mode > 2) return set_err(GOFFT_EINVAL, "dependent-launch mode must be 0, 1 or 2");
+  set_dependent_launch(mode);
+  return GOFFT_OK;
+}
 extern "C" int gofft_set_pipelined(int precision, int64_t n, int op, int on) {
   set_pipe_override(precision, n, op, on);
   return GOFFT_OK;

@@ -31,6 +31,7 @@
 #define GF_COLMAP 1        // thread mapping and smem layout across lines
 #define GF_FIRST_DIRECT 2  // first stage reads global memory
 #define GF_LAST_DIRECT 4   // last stage writes global memory
+#define GF_PDL_TRIGGER 16  // let the stream's next (dependent) launch start its CTAs early
 
 namespace gf {
 

@@ -51,10 +51,24 @@ GF_DEV void line_body(const KArgs &a, long long tile, bool active) {
   Op::template store<P>(a, line0);
 }
 
+// Programmatic dependent launch.  A line kernel launched with programmatic
+// stream serialization may be resident before the stream's previous kernel
+// has finished: it first waits until that grid has completed and its writes
+// are visible (griddepcontrol.wait; returns at once for a kernel launched
+// without the attribute, whose predecessors have already completed).  With
+// GF_PDL_TRIGGER it then allows the stream's next kernel to be scheduled
+// (griddepcontrol.launch_dependents): that kernel's CTAs take SMs as this
+// grid's last CTAs retire, and wait in their own griddepcontrol.wait.
+GF_DEV void pdl_enter(int flags) {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  if (flags & GF_PDL_TRIGGER) asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // The run-time-schedule kernel always uses the tile prologue / epilogue:
 // direct stages would multiply its (already long) body by four.
 template <class P, int MAXE, class Op>
 __global__ void __launch_bounds__(512, 1) k_line(const KArgs a) {
+  pdl_enter(a.flags);
   line_body<P, MAXE, Op>(a, blockIdx.x, true);
 }
 
@@ -222,6 +236,7 @@ template <class Op> constexpr bool row_fast() { return RowFast<Op>::value; }
 template <class P, int N, int T, int LPC, int MINB, class Op, class S>
 __global__ void __launch_bounds__(LPC *T, MINB) k_line_ct(const KArgs a) {
   using C = typename P::cpx;
+  pdl_enter(a.flags);
   const long long line0 = (long long)blockIdx.x * LPC;
   LineCtx c;
   if (a.flags & GF_COLMAP) {

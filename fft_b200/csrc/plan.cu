@@ -601,6 +601,14 @@ static std::atomic<int> g_pipe_on{0};
 void set_tma_pipeline(int on) { g_pipe_on.store(on ? 1 : 0); }
 int tma_pipeline() { return g_pipe_on.load(); }
 
+// Programmatic dependent launch of the line kernels (k_line_ct, k_line):
+// 0 off, 1 launched with programmatic stream serialization (each kernel
+// waits for its predecessor in griddepcontrol.wait), 2 also triggering the
+// next launch from every CTA's start.
+static std::atomic<int> g_pdl{0};
+void set_dependent_launch(int mode) { g_pdl.store(mode < 0 ? 0 : (mode > 2 ? 2 : mode)); }
+int dependent_launch() { return g_pdl.load(); }
+
 // The kernels' timeout word (set when a bounded wait gives up), one per
 // device in the library image: its address comes from cudaGetSymbolAddress,
 // so using it allocates nothing.
@@ -885,6 +893,7 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   // pipe choice, gofft_set_pipelined)
   const bool no_pipe = !get_pipe_override(dp.prec, dp.n, op);
   long long grid = (nlines + lpc - 1) / lpc;
+  bool pp = false;
   {
     // persistent double-buffered variant when two tile buffers fit
     if (!conv && !no_pipe && 2 * smem <= max_smem_optin() && grid > 2 * num_sms()) {
@@ -897,6 +906,7 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
         grid = std::min<long long>(grid, (long long)per_sm * num_sms());
         smem *= 2;
         a.flags &= ~GF_FIRST_DIRECT;
+        pp = true;
       }
     }
     if (!f) f = kernel_ct_for(dp, op, lpc, false);
@@ -916,13 +926,30 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
     cudaEventCreate(&rec.b);
     cudaEventRecord(rec.a, st);
   }
-  f<<<(unsigned)grid, lpc * dp.lp.T, smem, st>>>(a);
-  GF_CK(cudaGetLastError());
+  const int pdl = pp ? 0 : g_pdl.load();
+  if (pdl) {
+    if (pdl == 2) a.flags |= GF_PDL_TRIGGER;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)(lpc * dp.lp.T));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {&a};
+    GF_CK(cudaLaunchKernelExC(&cfg, (const void *)f, args));
+  } else {
+    f<<<(unsigned)grid, lpc * dp.lp.T, smem, st>>>(a);
+    GF_CK(cudaGetLastError());
+  }
   if (timed) {
     cudaEventRecord(rec.b, st);
     std::ostringstream k;
     k << op_name(op) << "/n=" << dp.n << "/prec=" << dp.prec << "/lpc=" << lpc << "/T=" << dp.lp.T
-      << "/flags=" << a.flags;
+      << "/flags=" << (a.flags & ~GF_PDL_TRIGGER);
     rec.key = k.str();
     rec.bytes = algo_bytes(op, dp, a, nlines);
     std::lock_guard<std::mutex> lk(g_tmu);

@@ -180,6 +180,8 @@ inline Side contig(void *p, long long len) { return mk_side(p, len, 0, 1, 1); }
 // device's timeout word: 0, or 4 (timeout) with the error text set.
 void set_tma_pipeline(int on);
 int tma_pipeline();
+void set_dependent_launch(int mode);
+int dependent_launch();
 int pipe_status(bool clear);
 
 // Instrumentation (launch counter, CUDA-event timing per line kernel).

@@ -16,7 +16,8 @@ uneven batch (4096 complex64 signals, lengths drawn from seed 2 over
 {60, 128, 360, 1000, 1009, 4096, 10007, 65536}) one class at a time.
 `spectrogram` is the fused spectrogram of an --n-sample signal (Hann 2048,
 overlap 1536); `filter2` the 2-D spectral filter forward then backward.
-`--pipe off` turns the TMA-fed persistent line kernel off for comparison.
+`--pipe off` turns the TMA-fed persistent line kernel off for comparison;
+`--pdl` sets the programmatic dependent-launch mode of the line kernels.
 """
 import argparse
 
@@ -72,11 +73,14 @@ def main():
     ap.add_argument("--pipe", default="on", choices=["on", "off"], help="TMA-fed persistent line kernel")
     ap.add_argument("--lanes", type=int, default=0, help="lanes of blocked plans (0: default)")
     ap.add_argument("--sched", default="", help="schedule variants, e.g. 1024:1,512:1")
+    ap.add_argument("--pdl", type=int, default=-1, help="dependent-launch mode 0/1/2 (-1: the default)")
     a = ap.parse_args()
     torch.cuda.set_device(0)
     from . import tune
     tune.set_tma_pipeline(a.pipe == "on")
     tune.set_lanes(a.lanes)
+    if a.pdl >= 0:
+        tune.set_dependent_launch(a.pdl)
     if a.wisdom:
         with open(a.wisdom) as f:
             tune.import_wisdom(f.read())

@@ -79,6 +79,13 @@ def set_tma_pipeline(on):
     check(lib().gofft_set_tma_pipeline(1 if on else 0))
 
 
+def set_dependent_launch(mode):
+    """Programmatic dependent launch of the line kernels made afterwards:
+    0 off, 1 each waits on the device for its predecessor, 2 also lets the
+    next one be scheduled early (results identical in every mode)."""
+    check(lib().gofft_set_dependent_launch(int(mode)))
+
+
 def pipeline_status():
     """Raises if a pipelined line kernel's bounded wait gave up since the
     last call (synchronises the device)."""

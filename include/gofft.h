@@ -337,6 +337,14 @@ GOFFT_API int gofft_set_tma_pipeline(int on);
  * bounded waits gave up since the last call (results of that launch are
  * then invalid).  No such wait gives up in normal operation. */
 GOFFT_API int gofft_pipeline_status(void);
+/* Programmatic dependent launch of the line kernels made afterwards: 0 off
+ * (each kernel starts when the stream's previous one has completed), 1 each
+ * line kernel may be scheduled before its predecessor in the stream has
+ * finished and waits on the device until it has (its writes visible), 2 as
+ * 1 with every line kernel also letting the next one be scheduled from the
+ * start of its CTAs.  Results are identical in every mode.  GOFFT_EINVAL for
+ * another mode. */
+GOFFT_API int gofft_set_dependent_launch(int mode);
 /* Selects (on = 1) the persistent double-buffered line kernel for
  * (precision, n, op) where one exists.  Used by the autotuner. */
 GOFFT_API int gofft_set_pipelined(int precision, int64_t n, int op, int on);
