@@ -48,7 +48,7 @@ def algo_bytes(prec_bytes):
 # of a launch over whole images (dram__bytes_read.sum + dram__bytes_write.sum,
 # caches flushed before the launch), divided by the images it covered; and
 # how many passes of each kernel a round trip makes over every image.
-DRAM_PER_IMAGE = {"c2c/n=1024/prec=0": 8425280, "r2c_packed/n=512/prec=0": 8406720}
+DRAM_PER_IMAGE = {"c2c/n=1024/prec=0": 8437376, "r2c_packed/n=512/prec=0": 8476032}
 PASSES = {"c2c": 2, "r2c_packed": 1, "c2r_packed": 1}
 
 

@@ -130,7 +130,9 @@ static int plan_ws(gofft_plan *p) {
   } else {
     // per lane: the block's spectrum buffer, then the passes' own workspace
     const long long rows = p->shape[0], rc = p->shape[1] / 2 + 1;
-    const size_t cols_buf = ((size_t)rows * rc * p->chunk * csize(p->prec) + 255) & ~(size_t)255;
+    // the tiled intermediate rounds the block's column-lines up to a whole group
+    const long long W = 64 / (long long)csize(p->prec);
+    const size_t cols_buf = ((size_t)rows * (rc * p->chunk + W - 1) * csize(p->prec) + 255) & ~(size_t)255;
     const size_t sub = std::max(p->rx->ws_bytes(rows * p->chunk), p->ax[0]->ws_bytes(rc * p->chunk));
     p->lane_buf = cols_buf;
     p->lane_bytes = (cols_buf + sub + 255) & ~(size_t)255;
@@ -426,33 +428,61 @@ static int exec_c2c(gofft_plan *p, const void *in, void *out, int inverse, cudaS
 }
 
 
-// One block of nb images of a rank-2 real forward, on stream s with the
-// lane's pass workspace wsx.
-static int r2c_block(gofft_plan *p, const char *src, char *dst, long long nb, char *wsx, cudaStream_t s,
-                     double wsc) {
+// Whether a rank-2 real plan keeps its row-to-column intermediate in the
+// tiled layout (TiledPos in ops.cuh): groups of W column-lines (64 bytes of
+// a row: 4 complex128 or 8 complex64), each a contiguous rows x W block, so
+// the column pass reads or writes whole contiguous tiles on that side
+// instead of one 64-byte row segment per row.  FP64 plans only: the FP32
+// forms measured slower tiled (32 x 1024^2 round trip 0.2664 ms image layout,
+// 0.2718 ms tiled, 0.2685 ms tiled forward only; their row passes lose more
+// than the column pass gains).  Packed fused row transforms only (even row
+// length, one CTA per row), and not while the opt-in TMA-fed kernel is on (it
+// reads and writes the image layout).
+static bool tiled_real2(const gofft_plan *p) {
+  return p->prec == F64 && p->rank == 2 && p->shape[0] > 1 && p->rx->can_tile() && !tma_pipeline();
+}
+
+// The column pass's view of the tiled intermediate: line L (image * rc +
+// column) starts at (L / W) * W * rows + L % W, elements W apart.
+static Side tiled_side(const gofft_plan *p, char *buf) {
+  const long long W = 64 / (long long)csize(p->prec), rows = p->shape[0];
+  return mk_side(buf, W * rows, 1, W, W);
+}
+
+// One block of nb images of a rank-2 real forward, on stream s: rows into the
+// lane's block buffer colbuf (tiled), columns from there into dst; wsx is the
+// lane's pass workspace.
+static int r2c_block(gofft_plan *p, const char *src, char *dst, long long nb, char *colbuf, char *wsx,
+                     cudaStream_t s, double wsc) {
   const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
-  // rows: real transform along the last axis (rfft2.go:41-51)
+  const Side cs = mk_side(dst, rows * rc, 1, rc, rc);
+  if (tiled_real2(p)) {
+    // rows: real transform along the last axis (rfft2.go:41-51)
+    if (int e = p->rx->r2c(contig((void *)src, cols), contig(colbuf, rc), nb * rows, wsx, s, wsc, rows)) return e;
+    // columns: complex transform down each of the rc columns (rfft2.go:53-72)
+    return p->ax[0]->exec(tiled_side(p, colbuf), cs, nb * rc, 0, 0, 1.0, wsx, s);
+  }
   if (int e = p->rx->r2c(contig((void *)src, cols), contig(dst, rc), nb * rows, wsx, s, wsc)) return e;
-  // columns: complex transform down each of the rc columns (rfft2.go:53-72)
   if (rows > 1) {
-    const Side cs = mk_side(dst, rows * rc, 1, rc, rc);
     if (int e = p->ax[0]->exec(cs, cs, nb * rc, 0, 0, 1.0, wsx, s)) return e;
   }
   return GOFFT_OK;
 }
 
 // One block of nb images of a rank-2 real inverse: columns into the lane's
-// block buffer colbuf, then the real rows into dst.
+// block buffer colbuf (tiled when the plan allows), then the real rows into
+// dst.
 static int c2r_block(gofft_plan *p, const char *src, char *dst, long long nb, char *colbuf, char *wsx,
                      cudaStream_t s, bool adj) {
   const long long rows = p->shape[0], cols = p->shape[1], rc = cols / 2 + 1;
+  const bool tiled = tiled_real2(p);
   // columns: complex inverse, normalised by 1/rows (rfft2.go:100-120)
   const Side cin = mk_side((void *)src, rows * rc, 1, rc, rc);
-  const Side cout = mk_side(colbuf, rows * rc, 1, rc, rc);
+  const Side cout = tiled ? tiled_side(p, colbuf) : mk_side(colbuf, rows * rc, 1, rc, rc);
   if (int e = p->ax[0]->exec(cin, cout, nb * rc, 1, 1, adj ? 1.0 : 1.0 / (double)rows, wsx, s)) return e;
   // rows: real inverse of length cols (rfft2.go:122-136)
   return p->rx->c2r(contig(colbuf, rc), (int)rc, contig(dst, cols), nb * rows, adj ? (double)cols : 1.0, wsx, s,
-                    adj);
+                    adj, tiled ? rows : 0);
 }
 
 // wsc != 0: the adjoint of the inverse (edge-bin weighting with scale wsc on
@@ -471,7 +501,7 @@ static int exec_r2c(gofft_plan *p, const void *in, void *out, cudaStream_t st, d
     const long long nb = std::min(p->chunk, p->batch - b0);
     const char *src = (const char *)in + (size_t)b0 * rows * cols * r;
     char *dst = (char *)out + (size_t)b0 * rows * rc * c;
-    if (int e = r2c_block(p, src, dst, nb, ln.sub(blk), ln.stream(blk), wsc)) return ln.join(e);
+    if (int e = r2c_block(p, src, dst, nb, ln.buf(blk), ln.sub(blk), ln.stream(blk), wsc)) return ln.join(e);
   }
   return ln.join(GOFFT_OK);
 }
@@ -629,7 +659,7 @@ static int host_run_real2(gofft_plan *p, const void *in, void *out, int which) {
       rc_ = set_err(GOFFT_ECUDA, std::string("host pipeline: ") + cudaGetErrorString(ce));
       break;
     }
-    rc_ = which == 1 ? r2c_block(p, din, dout, nb, buf + p->lane_buf, s, 0.0)
+    rc_ = which == 1 ? r2c_block(p, din, dout, nb, buf, buf + p->lane_buf, s, 0.0)
                      : c2r_block(p, din, dout, nb, buf, buf + p->lane_buf, s, false);
     if (rc_) break;
     ce = cudaEventRecord(done, s);

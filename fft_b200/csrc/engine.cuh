@@ -385,6 +385,45 @@ template <int N, int T, int R, int... Rs> constexpr int ct_maxe_r() {
 // offsets.
 template <int STEP, class C> GF_DEV C &slot(C *b, int i) { return b[spad(i) * STEP]; }
 
+// FP64 twiddles of one radix-4/8/16 butterfly from one to three table
+// entries.  Plane r-1 of a stage's table holds W^(k r); the other powers are
+// products of exactly rounded entries (w^2 = w*w, w^3 = w^2*w, ...: at most
+// three products deep, a few ulp), so a butterfly makes one load (three for
+// radix 16) where it made R-1.  Each table read is an L1/L2 round trip after
+// the stage's barrier; the products are FP64 work, which the line kernels
+// have spare.  Measured on the 1024-point FP64 column pass of 4 images:
+// 20.2 -> 18.7 us.
+template <class P, int R> constexpr bool tw_pow() {
+  return std::is_same<P, PrecF64>::value && (R == 4 || R == 8 || R == 16);
+}
+template <int R> GF_DEV void tw_apply_pow(double2 *x, const double2 *tw, int ns, int k) {
+  const double2 w1 = ld_keep(&tw[k]);
+  const double2 w2 = cmul(w1, w1), w3 = cmul(w2, w1);
+  x[1] = cmul(x[1], w1);
+  x[2] = cmul(x[2], w2);
+  x[3] = cmul(x[3], w3);
+  if constexpr (R == 8) {
+    const double2 w4 = cmul(w2, w2);
+    x[4] = cmul(x[4], w4);
+    x[5] = cmul(x[5], cmul(w4, w1));
+    x[6] = cmul(x[6], cmul(w4, w2));
+    x[7] = cmul(x[7], cmul(w4, w3));
+  } else if constexpr (R == 16) {
+    const double2 w4 = ld_keep(&tw[3 * ns + k]), w8 = ld_keep(&tw[7 * ns + k]);
+    const double2 w12 = cmul(w8, w4);
+    x[4] = cmul(x[4], w4);
+    x[8] = cmul(x[8], w8);
+    x[12] = cmul(x[12], w12);
+#pragma unroll
+    for (int r = 1; r < 4; r++) {
+      const double2 wr = r == 1 ? w1 : (r == 2 ? w2 : w3);
+      x[4 + r] = cmul(x[4 + r], cmul(w4, wr));
+      x[8 + r] = cmul(x[8 + r], cmul(w8, wr));
+      x[12 + r] = cmul(x[12 + r], cmul(w12, wr));
+    }
+  }
+}
+
 // The barrier between a stage's loads and its stores: the whole CTA, or (in
 // warp-specialised kernels) only the warps that work on the tile.
 struct CtaBar {
@@ -445,7 +484,9 @@ GF_DEV void stage_ct(typename P::cpx (&v)[E], typename P::cpx *sb, const KArgs &
     if (EXACT || j < NB) {
       const int q = j / NS, k = j % NS;
       if constexpr (NS > 1) {
-        if constexpr (short_tw<P, N>()) {
+        if constexpr (tw_pow<P, R>()) {
+          tw_apply_pow<R>(&v[b * R], tw, NS, k);
+        } else if constexpr (short_tw<P, N>()) {
 #pragma unroll
           for (int r = 1; r < R; r++) v[b * R + r] = cmul(v[b * R + r], ld_keep(&twh[(r - 1) * NS + k]));
         } else {

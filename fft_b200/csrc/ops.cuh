@@ -20,7 +20,11 @@
 // adjoints -- forward ops multiply bins 0 < k < n/2 (and k = n/2 for odd n)
 // by 2, inverse ops divide them by 2 as they are read.
 #define GF_EDGE_WEIGHT 0x20000000
-#define GF_IC_MASK 0x1fffffff
+// KArgs::ic bit of the packed real ops: the spectrum side is the tiled
+// intermediate of a rank-2 real transform (TiledPos below; ib = rows per
+// image, the side's Side is the identity, line_off(line) = line).
+#define GF_TILED 0x10000000
+#define GF_IC_MASK 0x0fffffff
 
 namespace gf {
 
@@ -48,6 +52,83 @@ template <class P> GF_DEV void load_real_pair(const KArgs &a, Cx<P> *dst, long l
     cp_async_n<sizeof(Rl)>(&dst->x, &in[base]);
     cp_async_n<sizeof(Rl)>(&dst->y, &in[base + st]);
   }
+}
+
+// The tiled intermediate of a rank-2 real transform (rows x bins half-spectra,
+// a block of images).  Column-line Lc = image * bins + bin is stored in
+// groups of W = 64 bytes / element size (4 complex128, 8 complex64): element
+// (Lc, row) at (Lc / W) * W * rows + W * row + Lc % W.  The W columns a
+// column-pass CTA transforms (its lines per CTA) are then one contiguous
+// rows x W block -- the image layout gave it one 64-byte row segment per row
+// and its loads waited on them -- and the row pass writes 64-byte runs.
+template <class P> constexpr int tile_lw() { return sizeof(Cx<P>) == 16 ? 2 : 3; }  // log2 W
+template <int LW> struct TiledPos {
+  long long lc0, rowW, rowsW;  // first column-line of the row's image, W * row, W * rows
+  GF_HD long long at(long long k) const {
+    const long long L = lc0 + k;
+    return (L >> LW) * rowsW + rowW + (L & ((1 << LW) - 1));
+  }
+};
+template <int LW> GF_HD TiledPos<LW> tiled_pos(long long line, long long rows, long long bins) {
+  const long long img = line / rows;
+  TiledPos<LW> t;
+  t.lc0 = img * bins;
+  t.rowW = (line - img * rows) << LW;
+  t.rowsW = rows << LW;
+  return t;
+}
+
+// Walks the tiled elements of the CTA's lines (bins 0..bins-1 of lines
+// line0..line0+lpc-1): f(l, k, off) for local line l, bin k and the element
+// offset in the tiled buffer.  When the CTA's lines lie in one image (rows
+// divisible by the lines per CTA, an even number of them) each warp takes two
+// lines x 16 consecutive bins: 32 / (2 W) groups, each a 128-byte contiguous
+// piece (two rows of W) of the group's run in global memory, and 16
+// consecutive slots of each line in shared memory, so the shared-memory side
+// is free of bank conflicts (a warp on four lines x W bins met a four-way
+// conflict through the line pitch).  Otherwise element by element.
+template <class P, class F> GF_DEV void tiled_loop(const KArgs &a, long long line0, int bins, F f) {
+  constexpr int LW = tile_lw<P>(), W = 1 << LW, NG = 32 / (2 * W);
+  const int L = a.lpc;
+  const long long rows = a.ib;
+  const int nw = (int)(blockDim.x >> 5), pairs = L >> 1;
+  if (rows % L == 0 && (L & 1) == 0 && (blockDim.x & 31) == 0 && nw % pairs == 0) {
+    const TiledPos<LW> tp = tiled_pos<LW>(line0, rows, bins);
+    const long long g0 = tp.lc0 >> LW;
+    const int ng = (int)(((tp.lc0 + bins - 1) >> LW) - g0 + 1);
+    const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
+    const int q = lane & (W - 1), r2 = (lane >> LW) & 1, gsub = lane >> (LW + 1);
+    const int l = 2 * (warp % pairs) + r2;
+    if (line0 + l >= a.nlines) return;
+    const int k0 = (int)((g0 << LW) - tp.lc0) + q;
+    const int bstep = nw / pairs;
+    // element (group g0 + gi, line l, column q): (g0 + gi) * W * rows + W * (row0 + l) + q
+    const long long base = g0 * tp.rowsW + tp.rowW + (l << LW) + q;
+    for (int gi = (warp / pairs) * NG + gsub; gi < ng; gi += bstep * NG) {
+      const int k = k0 + W * gi;
+      if (k < 0 || k >= bins) continue;
+      f(l, k, base + (long long)gi * tp.rowsW);
+    }
+    return;
+  }
+  for (int e = threadIdx.x; e < L * bins; e += blockDim.x) {
+    const int l = e / bins, k = e - l * bins;
+    if (line0 + l >= a.nlines) continue;
+    f(l, k, tiled_pos<LW>(line0 + l, rows, bins).at(k));
+  }
+}
+
+// Tiled bins 0..bins-1 (missing bins k >= nb zeroed) of the CTA's lines into
+// their line buffers.
+template <class P> GF_DEV void load_tiled(const KArgs &a, long long line0, int bins, int nb, void *sb) {
+  using C = Cx<P>;
+  using Rl = typename P::real;
+  const C *in = (const C *)a.in.ptr;
+  tiled_loop<P>(a, line0, bins, [&](int l, int k, long long off) {
+    C *d = &line_view<C>(a, l, sb)[k];
+    if (k < nb) cp_async_n<sizeof(C)>(d, &in[off]);
+    else *d = mkc((Rl)0, (Rl)0);
+  });
 }
 
 // Copies bins 0..min(nb, cnt)-1 of each line raw into slots 0.., zeroing the
@@ -210,16 +291,21 @@ struct OpR2CPacked {
     using Rl = typename P::real;
     Cx<P> *out = (Cx<P> *)a.out.ptr;
     const long long st = a.out.stride;
+    const bool tiled = (a.ic & GF_TILED) != 0;
+    const int m = a.lp.n;
+    // tiled: the out side is the identity, so base is the line index
+    auto at = [&](long long base, int k) {
+      return tiled ? tiled_pos<tile_lw<P>()>(base, a.ib, m + 1).at(k) : base + (long long)k * st;
+    };
     if (a.ic & GF_EDGE_WEIGHT) {
-      const int m = a.lp.n;
       const Rl sc = (Rl)a.scale;
       untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) {
         const Rl w = (k == 0 || k == m) ? sc : (Rl)2 * sc;
-        out[base + (long long)k * st] = mkc(v.x * w, v.y * w);
+        out[at(base, k)] = mkc(v.x * w, v.y * w);
       }, sb);
       return;
     }
-    untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) { out[base + (long long)k * st] = v; }, sb);
+    untangle_tile<P>(a, line0, [&](long long base, int k, Cx<P> v) { out[at(base, k)] = v; }, sb);
   }
   // Row-layout fast paths for the compiled-schedule kernels (M = lp.n, T
   // threads per line; thread c.t of line c.l, line data at sb).
@@ -232,7 +318,6 @@ struct OpR2CPacked {
     using C = Cx<P>;
     using Rl = typename P::real;
     using TW = typename P::tw_t;
-    if (!c.valid) return;
     constexpr int H = M / 2 + 1;
     constexpr int IT = (H + T - 1) / T;
     const TW *tw = (const TW *)a.aux0;
@@ -241,31 +326,43 @@ struct OpR2CPacked {
     const Rl half = (Rl)0.5;
     const bool wgt = (a.ic & GF_EDGE_WEIGHT) != 0;
     const Rl sc = (Rl)a.scale;
+    const bool tiled = (a.ic & GF_TILED) != 0;
+    // bins k and M - k from the packed spectrum's slots k and M - k
+    auto untangle = [&](auto emit) {
 #pragma unroll
-    for (int it = 0; it < IT; it++) {
-      const int k = c.t + it * T;
-      if (IT * T > H && k >= H) break;
-      if (k == 0) {
-        const C z0 = sb[0];
-        const Rl w = wgt ? sc : (Rl)1;
-        out[0] = mkc((z0.x + z0.y) * w, (Rl)0);
-        out[M * st] = mkc((z0.x - z0.y) * w, (Rl)0);
-        continue;
+      for (int it = 0; it < IT; it++) {
+        const int k = c.t + it * T;
+        if (IT * T > H && k >= H) break;
+        if (k == 0) {
+          const C z0 = sb[0];
+          const Rl w = wgt ? sc : (Rl)1;
+          emit(0, mkc((z0.x + z0.y) * w, (Rl)0));
+          emit(M, mkc((z0.x - z0.y) * w, (Rl)0));
+          continue;
+        }
+        const C zk = sb[spad(k)], zm = sb[spad(M - k)];
+        const C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
+        const C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
+        C t;
+        if constexpr (short_tw<P, M>()) t = cmul(xo, ld_keep(&((const float2 *)a.aux1)[k]));
+        else t = twmul(xo, ld_keep(&tw[k]));
+        C lo = cadd(xe, t), hi = mkc(xe.x - t.x, t.y - xe.y);
+        if (wgt) {
+          const Rl w2 = (Rl)2 * sc;
+          lo = mkc(lo.x * w2, lo.y * w2);
+          hi = mkc(hi.x * w2, hi.y * w2);
+        }
+        emit(k, lo);
+        if (M - k != k) emit(M - k, hi);
       }
-      const C zk = sb[spad(k)], zm = sb[spad(M - k)];
-      const C xe = mkc((zk.x + zm.x) * half, (zk.y - zm.y) * half);
-      const C xo = mkc((zk.y + zm.y) * half, (zm.x - zk.x) * half);
-      C t;
-      if constexpr (short_tw<P, M>()) t = cmul(xo, ld_keep(&((const float2 *)a.aux1)[k]));
-      else t = twmul(xo, ld_keep(&tw[k]));
-      C lo = cadd(xe, t), hi = mkc(xe.x - t.x, t.y - xe.y);
-      if (wgt) {
-        const Rl w2 = (Rl)2 * sc;
-        lo = mkc(lo.x * w2, lo.y * w2);
-        hi = mkc(hi.x * w2, hi.y * w2);
-      }
-      out[k * st] = lo;
-      if (M - k != k) out[(M - k) * st] = hi;
+    };
+    if (!c.valid) return;
+    if (tiled) {
+      const auto tp = tiled_pos<tile_lw<P>()>(c.line, a.ib, M + 1);
+      C *tout = (C *)a.out.ptr;
+      untangle([&](int kk, C v) { tout[tp.at(kk)] = v; });
+    } else {
+      untangle([&](int kk, C v) { out[kk * st] = v; });
     }
   }
 };
@@ -289,7 +386,8 @@ struct OpC2RPacked {
   }
   template <class P> static GF_DEV void load(const KArgs &a, long long line0, void *sb = nullptr) {
     const int m = a.lp.n;
-    load_bins<P>(a, line0, m + 1, a.ic & GF_IC_MASK, sb);
+    if (a.ic & GF_TILED) load_tiled<P>(a, line0, m + 1, a.ic & GF_IC_MASK, sb);
+    else load_bins<P>(a, line0, m + 1, a.ic & GF_IC_MASK, sb);
   }
   template <class P> static GF_DEV void prep(const KArgs &a, long long line0, void *sb = nullptr) {
     using C = Cx<P>;
@@ -338,10 +436,14 @@ struct OpC2RPacked {
   }
   // Row-layout fast paths for the compiled-schedule kernels (M = lp.n).
   static constexpr bool kRowFast = true;
-  template <class P, int M, int T> static GF_DEV void load_row(const KArgs &a, const LineCtx &c, long long) {
+  template <class P, int M, int T> static GF_DEV void load_row(const KArgs &a, const LineCtx &c, long long line0) {
     using C = Cx<P>;
     using Rl = typename P::real;
     constexpr int IT = (M + 1 + T - 1) / T;
+    if (a.ic & GF_TILED) {  // the whole CTA copies its lines' tiled runs
+      load_tiled<P>(a, line0, M + 1, a.ic & GF_IC_MASK, nullptr);
+      return;
+    }
     C *d = line_view<C>(a, c.l).b;
     if (!c.valid) return;
     const C *in = (const C *)a.in.ptr + c.ioff;

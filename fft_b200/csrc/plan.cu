@@ -872,7 +872,10 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   if (nlines <= 0) return 0;
   if (nlines >= (1ll << 31)) return set_err(5, "too many lines in one launch");
   if (op == OP_RADER_IP) return launch_rader_ip(dp, a, nlines, st);
-  if (!conv && lpc <= 0) {
+  // tiled real intermediates are read and written by the one-tile-per-CTA
+  // kernels only (the persistent variants do not know the layout)
+  const bool tiled = (op == OP_R2C || op == OP_C2R) && (a.ic & GF_TILED);
+  if (!conv && lpc <= 0 && !tiled) {
     int rc = 0;
     if (try_pipe(op, dp, a, nlines, st, &rc)) return rc;
   }
@@ -891,7 +894,7 @@ int launch_line(int op, const DevProg &dp, KArgs a, long long nlines, cudaStream
   // the persistent double-buffered variant halves resident CTAs; measured
   // slower on the 1024/512-point lines, so it is opt-in (the autotuner's
   // pipe choice, gofft_set_pipelined)
-  const bool no_pipe = !get_pipe_override(dp.prec, dp.n, op);
+  const bool no_pipe = tiled || !get_pipe_override(dp.prec, dp.n, op);
   long long grid = (nlines + lpc - 1) / lpc;
   bool pp = false;
   {
@@ -1484,19 +1487,22 @@ size_t ExecReal::ws_bytes(long long nl) const {
 }
 
 int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaStream_t st,
-                  double wsc) const {
+                  double wsc, long long tiled_rows) const {
   if (nl <= 0 || n == 0) return 0;
   const size_t c = csize(prec);
   const long long m = n / 2;
+  if (tiled_rows > 0 && mode != R_PACKED_FUSED) return set_err(5, "tiled bins need a packed fused real plan");
   switch (mode) {
     case R_PACKED_FUSED: {
       KArgs a{};
       a.in = in;
-      a.out = out;
+      a.out = tiled_rows > 0 ? mk_side(out.ptr, 1, 0, 1, 1) : out;
       a.aux0 = tw2;
       a.aux1 = tw2_hi;
       a.scale = wsc != 0.0 ? wsc : 1.0;
-      a.ic = (pairs_aligned(in, prec) ? GF_PAIR_ALIGNED : 0) | (wsc != 0.0 ? GF_EDGE_WEIGHT : 0);
+      a.ic = (pairs_aligned(in, prec) ? GF_PAIR_ALIGNED : 0) | (wsc != 0.0 ? GF_EDGE_WEIGHT : 0) |
+             (tiled_rows > 0 ? GF_TILED : 0);
+      a.ib = tiled_rows;
       return launch_line(OP_R2C, *cx->prog, a, nl, st);
     }
     case R_FULL_FUSED: {
@@ -1531,18 +1537,21 @@ int ExecReal::r2c(const Side &in, const Side &out, long long nl, void *ws, cudaS
 }
 
 int ExecReal::c2r(const Side &in, int nb, const Side &out, long long nl, double scale, void *ws,
-                  cudaStream_t st, bool halve) const {
+                  cudaStream_t st, bool halve, long long tiled_rows) const {
   if (nl <= 0 || n == 0) return 0;
   const size_t c = csize(prec);
   const long long m = n / 2;
+  if (tiled_rows > 0 && mode != R_PACKED_FUSED) return set_err(5, "tiled bins need a packed fused real plan");
   switch (mode) {
     case R_PACKED_FUSED: {
       KArgs a{};
-      a.in = in;
+      a.in = tiled_rows > 0 ? mk_side(in.ptr, 1, 0, 1, 1) : in;
       a.out = out;
       a.aux0 = tw2;
       a.aux1 = tw2_hi;
-      a.ic = nb | (pairs_aligned(out, prec) ? GF_PAIR_ALIGNED : 0) | (halve ? GF_EDGE_WEIGHT : 0);
+      a.ib = tiled_rows;
+      a.ic = nb | (pairs_aligned(out, prec) ? GF_PAIR_ALIGNED : 0) | (halve ? GF_EDGE_WEIGHT : 0) |
+             (tiled_rows > 0 ? GF_TILED : 0);
       a.scale = scale / (double)m;
       return launch_line(OP_C2R, *cx->prog, a, nl, st);
     }

@@ -128,13 +128,17 @@ struct ExecReal {
   size_t ws_bytes(long long nlines) const;
   // in: reals, out: bins.  wsc != 0 applies the real-spectrum edge-bin
   // weighting of the adjoints: bins 0 and n/2 times wsc, the others 2 wsc.
+  // tiled_rows > 0: the bins side is the tiled intermediate of a rank-2
+  // transform with that many rows per image (its Side's pointer is used,
+  // nothing else); only packed fused plans (can_tile()) take it.
   int r2c(const Side &in, const Side &out, long long nlines, void *ws, cudaStream_t st,
-          double wsc = 0.0) const;
+          double wsc = 0.0, long long tiled_rows = 0) const;
   // in: bins (nb available per line), out: reals; the result is the
   // reference-normalised inverse (1/n) times `scale`.  halve: bins other than
   // 0 and n/2 enter halved (the adjoint of the forward's weighting).
   int c2r(const Side &in, int nb, const Side &out, long long nlines, double scale, void *ws,
-          cudaStream_t st, bool halve = false) const;
+          cudaStream_t st, bool halve = false, long long tiled_rows = 0) const;
+  bool can_tile() const { return mode == R_PACKED_FUSED; }
   std::string describe() const;
 };
 

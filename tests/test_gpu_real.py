@@ -114,6 +114,33 @@ def test_batched_rfft2_config2_shape():
     assert np.max(np.abs(back - x)) < 1e-12
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32mixed"])
+@pytest.mark.parametrize("shape,batch", [((1000, 64), 3), ((6, 720), 5), ((24, 512), 7), ((10, 30), 9),
+                                         ((1024, 1024), 3), ((5, 8), 11)])
+def test_rfft2_tiled_intermediate(prec, shape, batch):
+    """Batched FP64 rank-2 real transforms keep the row-to-column intermediate
+    in groups of four column-lines (the FP32 forms keep the image layout);
+    image boundaries fall inside groups (rc not a multiple of 4), rows need
+    not divide by the lines per CTA, and row lengths without a compiled
+    kernel (720 = 2 x 360) take the run-time kernel.  Each image must match
+    the oracle and invert to the input."""
+    from fft_b200.device import DevicePlan
+    R, C = shape
+    K = C // 2 + 1
+    tol = F64_TOL if prec == "f64" else F32_TOL
+    g = rng(R * 7 + C + batch)
+    x = g.standard_normal((batch, R, C))
+    dt = np.float64 if prec == "f64" else np.float32
+    p = DevicePlan("r2c", prec, [R, C], batch=batch)
+    X = p.r2c(torch.from_numpy(x.astype(dt)).cuda().reshape(batch, -1))
+    got = X.cpu().numpy().reshape(batch, R * K)
+    for b in range(batch):
+        assert rel_l2(got[b], O.rfft2(x[b], R, C)) <= tol
+    back = p.c2r(X).cpu().numpy().reshape(batch, R, C)
+    for b in range(batch):
+        assert rel_l2(back[b], x[b]) <= (1e-13 if prec == "f64" else 2 * F32_TOL)
+
+
 @pytest.mark.parametrize("pinned", [True, False])
 def test_batched_rfft2_host_pipeline(pinned):
     # host-buffer RFFT2/IRFFT2 of a batch spanning several blocks on both
